@@ -1,0 +1,401 @@
+#!/usr/bin/env python
+"""Spin-flip attempts/s of the B200 simulated-annealing sampler.
+
+Workload: the uneven batch -- 512 independent random-regular Ising problems,
+n ~ U[64, 4096], degree ~ U{3..16}, J ~ N(0,1), h ~ N(0,0.1), reads ~ U[32,1024],
+sweeps ~ U[256,2048], geometric beta 0.1 -> 5.0, Metropolis, sequential order,
+seeded synthetic data.  One step = one anneal of the whole batch (every read of
+every problem).  The persistent kernel (one launch, device work queue) is the
+headline; the plain one-launch-per-problem kernel is timed beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank anneals its own full batch (weak scaling, no
+collective on the data path); timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import copy
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "dwave-samplers_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+from b200sa import workloads  # noqa: E402
+
+METRIC = "spin-flip attempts/s, 1 B200: batched vs plain (bit-exact); BM grad steps/s"
+UNIT = "attempts/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--problems", type=int, default=512)
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-budget", type=float, default=15.0,
+                    help="seconds of CPU baseline sampling on rank 0")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args, rank=0):
+    probs = workloads.uneven_batch(num_problems=args.problems)
+    if rank:  # weak scaling: same shapes, rank-specific read seeds
+        for p in probs:
+            p.seeds = p.seeds + np.uint64(rank * (1 << 32))
+    return probs
+
+
+def workload_config(args, probs):
+    return {
+        "workload": f"uneven batch: {len(probs)} random-regular Ising problems, n~U[64,4096], "
+                    "degree~U{3..16}, J~N(0,1), h~N(0,0.1), reads~U[32,1024], "
+                    "sweeps~U[256,2048], geometric beta 0.1->5.0, Metropolis, sequential",
+        "problems": len(probs),
+        "reads": int(sum(p.num_reads for p in probs)),
+        "attempts_per_step": int(sum(p.attempts for p in probs)),
+        "max_n": int(max(p.n for p in probs)),
+        "l2": "inputs larger than L2 (packed problems + states exceed 126 MB)",
+        "seeds": "per read: base_seed + r",
+    }
+
+
+# ---------------------------------------------------------------- CPU side --
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_sample(probs, budget_s, threads=None, max_reads=None):
+    """Time the reference's own CPU implementation (the extension built from
+    its sources) -- or the C restatement when that build is absent -- on a
+    bounded sample of reads of the same workload, all host threads, one read
+    per call (num_samples=1, seed = that read's seed)."""
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    threads = threads or cpu_threads()
+    ref = oracle.reference_module()
+    kind = "reference" if ref is not None else "port"
+    rng = np.random.default_rng(99)
+    order = [(int(p), 0) for p in rng.permutation(len(probs))]
+    lists = {}
+
+    def one(item):
+        p, r = item
+        P = probs[p]
+        if ref is not None:
+            if p not in lists:
+                lists[p] = (list(map(float, P.h)), list(map(int, P.u)), list(map(int, P.v)),
+                            list(map(float, P.J)))
+            h, u, v, J = lists[p]
+            ref.simulated_annealing(1, h, u, v, J, P.sweeps_per_beta, P.betas, int(P.seeds[r]),
+                                    P.states[r:r + 1].copy())
+        else:
+            oracle.run(P.h, P.u, P.v, P.J, P.states[r:r + 1], P.sweeps_per_beta, P.betas,
+                       P.seeds[r:r + 1])
+        return P.sweeps_per_beta * len(P.betas) * P.n
+
+    # Python-list conversion outside the timed region.
+    if ref is not None:
+        for p, _ in order[: 4 * threads]:
+            P = probs[p]
+            lists[p] = (list(map(float, P.h)), list(map(int, P.u)), list(map(int, P.v)),
+                        list(map(float, P.J)))
+    attempts = 0
+    reads = 0
+    i = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while i < len(order):
+            if max_reads is not None and reads >= max_reads:
+                break
+            chunk = order[i:i + threads]
+            i += len(chunk)
+            attempts += sum(ex.map(one, chunk))
+            reads += len(chunk)
+            if max_reads is None and time.perf_counter() - t0 >= budget_s:
+                break
+    dt = time.perf_counter() - t0
+    return {"value": attempts / dt, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{reads} reads (read 0 of randomly chosen problems of the same batch, "
+                      f"full schedules), {attempts:.3e} attempts in {dt:.1f} s",
+            "seconds": dt, "attempts": attempts}
+
+
+# ------------------------------------------------------------- GPU helpers --
+
+class Clocks:
+    """Samples SM clock and throttle reasons with nvidia-smi while running."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        load = [x for x in sm if mx and x > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def algorithmic_bytes(probs, flips):
+    """Bytes the sweep must touch per launch (per-read state model):
+    initial delta energies n*(8 + 13*d), per attempt 9 (delta energy 8 + spin 1),
+    per flip 29*d + 9 (d x (index 4 + coupling 8 + neighbour spin 1 + delta
+    energy read-modify-write 16) + own spin and delta energy), and the final
+    energy 9n + 14m."""
+    fixed = 0.0
+    deg_w = 0.0
+    att = 0.0
+    for p in probs:
+        n, m, R = p.n, p.J.shape[0], p.num_reads
+        d = 2.0 * m / max(n, 1)
+        a = p.attempts
+        fixed += R * (n * (8 + 13 * d) + 9 * n + 14 * m) + 9 * a
+        deg_w += d * a
+        att += a
+    dbar = deg_w / max(att, 1)
+    return fixed + flips * (29 * dbar + 9)
+
+
+def h2d_d2h_bytes(probs):
+    bi = bo = 0
+    for p in probs:
+        n, m, R, nb = p.n, p.J.shape[0], p.num_reads, len(p.betas)
+        # packed arena (row, col, w, h, vinfo, COO, betas, thresholds), seeds,
+        # work items and initial states
+        bi += 4 * (n + 1) + 24 * m + 8 * n + n + 16 * m + 16 * nb + 8 * R + 16 * R + n * R
+        bo += n * R + 8 * R
+    return bi, bo
+
+
+# ------------------------------------------------------------------ arms ----
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    probs = workload(args)
+    threads = cpu_threads()
+    per_step = max(threads, 2 * threads)
+    for _ in range(args.warmup):
+        cpu_sample(probs, 0, threads, max_reads=threads)
+    t_att = 0
+    t_sec = 0.0
+    last = None
+    for k in range(args.steps):
+        r = cpu_sample(probs[k % 2::2] if k % 2 else probs, 0, threads, max_reads=per_step)
+        t_att += r["attempts"]
+        t_sec += r["seconds"]
+        last = r
+    value = t_att / t_sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * t_sec / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, probs),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": last["kind"],
+                         "sample": f"each step: {per_step} reads of the batch, one read per call "
+                                   "(num_samples=1, that read's seed), all host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from b200sa import Plan, sample_batch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    probs = workload(args, rank)
+    attempts = int(sum(p.attempts for p in probs))
+    plan = Plan(probs, device=local)
+    host_states = np.concatenate([p.states.ravel() for p in probs])
+    sin = torch.from_numpy(host_states).cuda()
+    sout = torch.empty_like(sin)
+    en = torch.empty(plan.total_reads, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def timed(mode, warmup, steps):
+        for _ in range(warmup):
+            plan.run(sin, sout, en, mode=mode, stream=stream, sync=False)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            plan.run(sin, sout, en, mode=mode, stream=stream, sync=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        return e0.elapsed_time(e1)
+
+    with Clocks(local) as clk:
+        total_ms = timed("persistent", args.warmup, args.steps)
+    total_ms = max_over_ranks(total_ms)
+    ms_step = total_ms / args.steps
+    value = world * attempts / (ms_step / 1000.0)
+
+    # Counters of one run (deterministic for these inputs).
+    stats = plan.run(sin, sout, en, mode="persistent", stream=stream, sync=True)
+    flips = stats["flips"]
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(args, probs) | {"parallelism": f"independent batch per GPU x{world}"},
+    }
+    peak, peak_src = measured_hbm_peak()
+    abytes = algorithmic_bytes(probs, flips)
+    achieved = abytes / (ms_step / 1000.0) / 1e9
+    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "traffic": None,
+                        "peak_source": peak_src,
+                        "algorithmic_bytes_per_launch": abytes}
+    line["clocks"] = clk.summary()
+    line["gpu_launches"] = args.steps
+    line["counters"] = {"flips": flips, "near_ties": stats["near_ties"],
+                        "attempts_per_pass": attempts / max(stats["passes"], 1)}
+
+    if not args.no_plain:
+        plain_ms = max_over_ranks(timed("plain", 1, args.plain_steps)) / args.plain_steps
+        line["plain"] = {"value": world * attempts / (plain_ms / 1000.0), "ms_per_step": plain_ms,
+                         "launches_per_step": len(probs)}
+        line["batched_over_plain"] = plain_ms / ms_step
+
+    # End to end through the C ABI with host buffers (pack + H2D + anneal + D2H).
+    bi, bo = h2d_d2h_bytes(probs)
+    e2e_times = []
+    for _ in range(args.e2e_steps + 1):
+        work = [copy.copy(p) for p in probs]
+        for w in work:
+            w.states = w.states.copy()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        sample_batch(work, mode="persistent", device=local)
+        dt = time.perf_counter() - t0
+        e2e_times.append(max_over_ranks(dt))
+    e2e = statistics.median(e2e_times[1:])
+    line["e2e"] = {"value": world * attempts / e2e, "unit": UNIT, "h2d_bytes_per_step": bi,
+                   "d2h_bytes_per_step": bo, "seconds_per_step": e2e}
+
+    if rank == 0 and not args.no_cpu:
+        cb = cpu_sample(probs, args.cpu_budget)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    plan.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

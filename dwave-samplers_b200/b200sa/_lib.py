@@ -1,0 +1,133 @@
+"""ctypes binding of libb200sa.so (C ABI in include/b200sa.h).
+
+The library is built in-tree by ``dwave-samplers_b200/build.py``.  There is no
+fallback: if the library is missing or cannot load, every sampling call
+raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libb200sa.so")
+
+OK = 0
+EINVAL = -1
+ECUDA = -2
+ENOMEM = -3
+ENODEV = -4
+ETIMEOUT = -5
+
+GIBBS = 0
+METROPOLIS = 1
+SEQUENTIAL = 0
+RANDOM = 1
+
+MODE_PERSISTENT = 0
+MODE_PLAIN = 1
+
+EXPORTS = (
+    "b200sa_sample",
+    "b200sa_sample_batch",
+    "b200sa_plan_create",
+    "b200sa_plan_layout",
+    "b200sa_plan_run",
+    "b200sa_plan_destroy",
+    "b200sa_version",
+)
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("reads", ctypes.c_int64),
+        ("attempts", ctypes.c_int64),
+        ("flips", ctypes.c_int64),
+        ("near_ties", ctypes.c_int64),
+        ("passes", ctypes.c_int64),
+        ("kernel_ms", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Problem(ctypes.Structure):
+    _fields_ = [
+        ("num_vars", ctypes.c_int32),
+        ("h", ctypes.c_void_p),
+        ("num_couplers", ctypes.c_int64),
+        ("coupler_starts", ctypes.c_void_p),
+        ("coupler_ends", ctypes.c_void_p),
+        ("coupler_weights", ctypes.c_void_p),
+        ("num_reads", ctypes.c_int32),
+        ("states", ctypes.c_void_p),
+        ("energies", ctypes.c_void_p),
+        ("sweeps_per_beta", ctypes.c_int32),
+        ("num_betas", ctypes.c_int32),
+        ("beta_schedule", ctypes.c_void_p),
+        ("seeds", ctypes.c_void_p),
+        ("varorder", ctypes.c_int32),
+        ("proposal", ctypes.c_int32),
+    ]
+
+
+INTERRUPT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the CUDA library, failing loudly when it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            f"{LIB_PATH} is not built; run `python dwave-samplers_b200/build.py`")
+    L = ctypes.CDLL(LIB_PATH)
+    c = ctypes
+    L.b200sa_sample.restype = c.c_int
+    L.b200sa_sample.argtypes = [
+        c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p,
+        c.c_int32, c.c_void_p, c.c_void_p, c.c_int32, c.c_int32, c.c_void_p,
+        c.c_void_p, c.c_int32, c.c_int32, c.c_int32, INTERRUPT_FN, c.c_void_p,
+        c.c_int32, c.POINTER(Stats), c.c_char_p, c.c_size_t]
+    L.b200sa_sample_batch.restype = c.c_int
+    L.b200sa_sample_batch.argtypes = [
+        c.POINTER(Problem), c.c_int32, c.c_int32, c.c_int32, c.POINTER(Stats),
+        c.c_char_p, c.c_size_t]
+    L.b200sa_plan_create.restype = c.c_int
+    L.b200sa_plan_create.argtypes = [
+        c.POINTER(Problem), c.c_int32, c.c_int32, c.POINTER(c.c_void_p),
+        c.c_char_p, c.c_size_t]
+    L.b200sa_plan_layout.restype = c.c_int
+    L.b200sa_plan_layout.argtypes = [c.c_void_p, c.c_void_p, c.c_void_p]
+    L.b200sa_plan_run.restype = c.c_int
+    L.b200sa_plan_run.argtypes = [
+        c.c_void_p, c.c_int32, c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p,
+        c.c_void_p, c.c_int32, c.POINTER(Stats), c.c_char_p, c.c_size_t]
+    L.b200sa_plan_destroy.restype = c.c_int
+    L.b200sa_plan_destroy.argtypes = [c.c_void_p]
+    L.b200sa_version.restype = c.c_char_p
+    L.b200sa_version.argtypes = []
+    _lib = L
+    return L
+
+
+def check(rc: int, err: ctypes.Array) -> int:
+    """Map a negative return code to the matching Python exception."""
+    if rc >= 0:
+        return rc
+    msg = err.value.decode(errors="replace") if err is not None else ""
+    if rc == EINVAL:
+        raise ValueError(msg or "invalid argument")
+    if rc == ENOMEM:
+        raise MemoryError(msg or "out of memory")
+    if rc == ETIMEOUT:
+        raise TimeoutError(msg or "device wait timed out")
+    raise RuntimeError(f"b200sa error {rc}: {msg}")
+
+
+def errbuf() -> ctypes.Array:
+    return ctypes.create_string_buffer(512)

@@ -1,0 +1,128 @@
+// Host-side packing: argument validation, order-preserving adjacency,
+// per-variable speculation info and the RNG jump matrix.
+#include "pack.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+
+#include "sa_types.h"
+
+namespace b200sa {
+
+int validate_problem(const b200sa_problem &p, std::string &msg) {
+    char buf[256];
+    if (p.num_vars < 0 || p.num_couplers < 0 || p.num_reads < 0) {
+        msg = "negative size";
+        return B200SA_EINVAL;
+    }
+    if (p.num_couplers > (int64_t)INT32_MAX / 2) {
+        msg = "too many couplers";
+        return B200SA_EINVAL;
+    }
+    if (p.num_vars > 0 && !p.h) {
+        msg = "h is NULL";
+        return B200SA_EINVAL;
+    }
+    if (p.num_couplers > 0 &&
+        (!p.coupler_starts || !p.coupler_ends || !p.coupler_weights)) {
+        msg = "coupler arrays are NULL";
+        return B200SA_EINVAL;
+    }
+    if (p.sweeps_per_beta < 0 || p.num_betas < 0 ||
+        (p.num_betas > 0 && !p.beta_schedule)) {
+        msg = "bad beta schedule";
+        return B200SA_EINVAL;
+    }
+    if (p.varorder != B200SA_SEQUENTIAL && p.varorder != B200SA_RANDOM) {
+        msg = "varorder must be 0 (sequential) or 1 (random)";
+        return B200SA_EINVAL;
+    }
+    if (p.proposal != B200SA_GIBBS && p.proposal != B200SA_METROPOLIS) {
+        msg = "proposal must be 0 (Gibbs) or 1 (Metropolis)";
+        return B200SA_EINVAL;
+    }
+    // cpu_sa.cpp:302-304 (the reference throws; here it is an error code).
+    for (int64_t c = 0; c < p.num_couplers; ++c) {
+        const int32_t a = p.coupler_starts[c], b = p.coupler_ends[c];
+        if (a < 0 || b < 0 || a >= p.num_vars || b >= p.num_vars) {
+            std::snprintf(buf, sizeof(buf),
+                          "coupler indexes contain an invalid variable "
+                          "(coupler %lld: %d, %d; num_vars %d)",
+                          (long long)c, a, b, p.num_vars);
+            msg = buf;
+            return B200SA_EINVAL;
+        }
+    }
+    return B200SA_OK;
+}
+
+void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
+    const int32_t n = p.num_vars;
+    const int64_t m = p.num_couplers;
+    out.row.assign((size_t)n + 1, 0);
+    out.col.resize((size_t)(2 * m));
+    out.w.resize((size_t)(2 * m));
+    out.vinfo.assign((size_t)n, 0);
+    for (int64_t c = 0; c < m; ++c) {
+        out.row[(size_t)p.coupler_starts[c] + 1]++;
+        out.row[(size_t)p.coupler_ends[c] + 1]++;
+    }
+    for (int32_t i = 0; i < n; ++i) out.row[i + 1] += out.row[i];
+    // Counting-sort fill in coupler order: the same per-variable order as the
+    // reference's push_back loop (cpu_sa.cpp:298-316).
+    std::vector<int32_t> cur(out.row.begin(), out.row.end() - 1);
+    for (int64_t c = 0; c < m; ++c) {
+        const int32_t a = p.coupler_starts[c], b = p.coupler_ends[c];
+        const double J = p.coupler_weights[c];
+        int32_t k = cur[a]++;
+        out.col[k] = b;
+        out.w[k] = J;
+        k = cur[b]++;
+        out.col[k] = a;
+        out.w[k] = J;
+    }
+    // Speculation info: nearest later neighbour and repeated targets.
+    std::vector<int32_t> mark((size_t)n, -1);
+    int32_t maxdeg = 0;
+    bool any_dup = false;
+    for (int32_t v = 0; v < n; ++v) {
+        int32_t dist = 32;
+        bool dup = false;
+        const int32_t e0 = out.row[v], e1 = out.row[v + 1];
+        maxdeg = std::max(maxdeg, e1 - e0);
+        for (int32_t e = e0; e < e1; ++e) {
+            const int32_t u = out.col[e];
+            if (u > v) dist = std::min(dist, u - v);
+            if (mark[u] == v) dup = true;
+            mark[u] = v;
+        }
+        out.vinfo[v] = (uint8_t)((dist & kDistMask) | (dup ? kDupFlag : 0));
+        any_dup |= dup;
+    }
+    out.max_degree = maxdeg;
+    out.any_dup = any_dup;
+}
+
+// One xorshift128+ state transition (cpu_sa.cpp:27-34 without the output).
+static inline void xs_advance(uint64_t &s0, uint64_t &s1) {
+    uint64_t a = s0;
+    const uint64_t b = s1;
+    s0 = b;
+    a ^= a << 23;
+    s1 = a ^ b ^ (a >> 17) ^ (b >> 26);
+}
+
+void rng_jump_columns(int64_t steps, uint32_t out[128][4]) {
+    for (int bit = 0; bit < 128; ++bit) {
+        uint64_t s0 = bit < 64 ? (1ull << bit) : 0;
+        uint64_t s1 = bit < 64 ? 0 : (1ull << (bit - 64));
+        for (int64_t k = 0; k < steps; ++k) xs_advance(s0, s1);
+        out[bit][0] = (uint32_t)s0;
+        out[bit][1] = (uint32_t)(s0 >> 32);
+        out[bit][2] = (uint32_t)s1;
+        out[bit][3] = (uint32_t)(s1 >> 32);
+    }
+}
+
+}  // namespace b200sa

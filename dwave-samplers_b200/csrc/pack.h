@@ -1,0 +1,33 @@
+// Host-side packing of one Ising problem into the device layout.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "b200sa.h"
+
+namespace b200sa {
+
+struct PackedAdjacency {
+    std::vector<int32_t> row;    // n+1
+    std::vector<int32_t> col;    // 2m
+    std::vector<double> w;       // 2m
+    std::vector<uint8_t> vinfo;  // n
+    int32_t max_degree = 0;
+    bool any_dup = false;
+};
+
+// Validates one problem's arguments (lengths, indices, enums).  Returns
+// B200SA_OK or B200SA_EINVAL with a message.
+int validate_problem(const b200sa_problem &p, std::string &msg);
+
+// Order-preserving adjacency, same order as cpu_sa.cpp:298-316.
+void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out);
+
+// Columns of the GF(2) matrix that advances an xorshift128+ state by `steps`
+// steps: column b is the state reached from the unit state with only bit b
+// set (bits 0-63 = word 0, 64-127 = word 1).  Four uint32 words per column:
+// word0 lo, word0 hi, word1 lo, word1 hi.
+void rng_jump_columns(int64_t steps, uint32_t out[128][4]);
+
+}  // namespace b200sa

@@ -1,0 +1,675 @@
+// C ABI of the B200 simulated-annealing sampler (declared in include/b200sa.h).
+//
+// Host side of the drop-in for general_simulated_annealing
+// (dwave/samplers/sa/src/cpu_sa.cpp:253-362): validation, order-preserving
+// packing, device residency, launch configuration, interrupt polling in read
+// order, and error codes in place of the reference's thrown exceptions.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "b200sa.h"
+#include "pack.h"
+#include "sa_launch.h"
+#include "sa_types.h"
+
+using namespace b200sa;
+
+namespace {
+
+int set_err(char *err, size_t errlen, int code, const std::string &msg) {
+    if (err && errlen > 0) {
+        std::snprintf(err, errlen, "%s", msg.c_str());
+    }
+    return code;
+}
+
+#define B200SA_CUDA(call)                                                        \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess)                                                   \
+            return set_err(err, errlen, B200SA_ECUDA,                            \
+                           std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() { cudaGetDevice(&prev); }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+int select_device(int device, cudaDeviceProp &prop, char *err, size_t errlen) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return set_err(err, errlen, B200SA_ENODEV, "no CUDA device available");
+    }
+    if (device < 0 || device >= count)
+        return set_err(err, errlen, B200SA_ENODEV,
+                       "device index " + std::to_string(device) + " out of range");
+    B200SA_CUDA(cudaSetDevice(device));
+    B200SA_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10)
+        return set_err(err, errlen, B200SA_ENODEV,
+                       std::string("this library is built for sm_100a (B200); device is ") +
+                           prop.name + " sm_" + std::to_string(prop.major * 10 + prop.minor));
+    return B200SA_OK;
+}
+
+template <typename T>
+struct DevArray {
+    T *ptr = nullptr;
+    size_t count = 0;
+    DevArray() = default;
+    DevArray(const DevArray &) = delete;
+    DevArray &operator=(const DevArray &) = delete;
+    ~DevArray() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        release();
+        count = n;
+        if (n == 0) return cudaSuccess;
+        return cudaMalloc(reinterpret_cast<void **>(&ptr), n * sizeof(T));
+    }
+};
+
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+const uint32_t (*jump_columns())[4] {
+    static uint32_t cols[128][4];
+    static bool ready = false;
+    if (!ready) {  // idempotent; concurrent first calls write identical values
+        rng_jump_columns(kHalf, cols);
+        ready = true;
+    }
+    return cols;
+}
+
+}  // namespace
+
+struct b200sa_plan_s {
+    int device = 0;
+    cudaDeviceProp prop{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int num_problems = 0;
+    std::vector<ProblemDev> hprobs;
+    std::vector<int32_t> n, reads, sweeps;  // per problem
+    std::vector<int64_t> state_off, read_off;
+    int64_t total_state = 0, total_reads = 0;
+    int32_t max_n = 0;
+    DevArray<uint8_t> arena;
+    DevArray<ProblemDev> dprobs;
+    DevArray<uint64_t> dseeds;
+    DevArray<ReadStats> dstats;
+    DevArray<int64_t> items_lpt, items_plain;
+    DevArray<unsigned long long> qhead;
+    DevArray<double> scratch_de;
+    DevArray<int8_t> scratch_s;
+    DevArray<uint64_t> carry;
+    int64_t scratch_stride = 0, scratch_slots = 0;
+    std::vector<int64_t> plain_item_off;  // per problem offset into items_plain
+
+    ~b200sa_plan_s() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+struct LaunchShape {
+    int cap_n;         // largest n kept in shared memory
+    int warps_per_cta;
+    int region;
+    int grid;
+};
+
+// Chooses how many warps share a CTA and which problems keep their state in
+// shared memory.  Every warp anneals one read at a time; a warp's shared
+// region holds the RNG ring plus, when n <= cap_n, the read's delta energies
+// and spins.  Larger problems keep those in a global slot (L2-resident).
+int shape_for(b200sa_plan_s *P, int32_t max_n_here, int64_t items, bool persistent,
+              LaunchShape &out, char *err, size_t errlen) {
+    const int smem_sm = (int)P->prop.sharedMemPerMultiprocessor;
+    const int smem_blk = (int)P->prop.sharedMemPerBlockOptin;
+    // Keep at least 4 resident warps per SM when the state lives on chip.
+    int cap = max_n_here;
+    if (region_bytes_for(cap) * 4 > smem_sm) cap = 0;
+    const int region = region_bytes_for(cap);
+    int w = std::max(1, std::min(kMaxThreadsPerCta / 32, smem_blk / region));
+    if (!persistent) w = std::min<int64_t>(w, std::max<int64_t>(1, items));
+    int per_sm = 0;
+    B200SA_CUDA(kernel_occupancy(w, region, &per_sm));
+    if (per_sm < 1) return set_err(err, errlen, B200SA_ECUDA, "kernel does not fit on an SM");
+    int grid;
+    if (persistent) {
+        grid = P->prop.multiProcessorCount * per_sm;
+        const int64_t need = (items + w - 1) / w;
+        grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, need));
+    } else {
+        grid = (int)std::max<int64_t>(1, (items + w - 1) / w);
+    }
+    out.cap_n = cap;
+    out.warps_per_cta = w;
+    out.region = region;
+    out.grid = grid;
+    return B200SA_OK;
+}
+
+int ensure_scratch(b200sa_plan_s *P, int64_t slots, int64_t stride, char *err,
+                   size_t errlen) {
+    stride = (stride + 15) & ~int64_t(15);
+    if (slots <= P->scratch_slots && stride <= P->scratch_stride) return B200SA_OK;
+    slots = std::max(slots, P->scratch_slots);
+    stride = std::max(stride, P->scratch_stride);
+    B200SA_CUDA(P->scratch_de.alloc((size_t)(slots * stride)));
+    B200SA_CUDA(P->scratch_s.alloc((size_t)(slots * stride)));
+    P->scratch_slots = slots;
+    P->scratch_stride = stride;
+    return B200SA_OK;
+}
+
+LaunchArgs base_args(b200sa_plan_s *P, const int8_t *in, int8_t *out, double *en,
+                     const uint64_t *seeds) {
+    LaunchArgs a{};
+    a.problems = P->dprobs.ptr;
+    a.states_in = in;
+    a.states_out = out;
+    a.energies = en;
+    a.seeds = seeds ? seeds : P->dseeds.ptr;
+    a.stats = P->dstats.ptr;
+    return a;
+}
+
+// Runs the items [first, first+count) of problem `pi`'s read-ordered list (plain
+// list) or the whole LPT list (persistent) with one launch.
+int launch_items(b200sa_plan_s *P, LaunchArgs a, const int64_t *items, int64_t count,
+                 int32_t max_n_here, bool persistent, bool shared_stream,
+                 cudaStream_t st, char *err, size_t errlen) {
+    if (count <= 0) return B200SA_OK;
+    LaunchShape s{};
+    int rc = shape_for(P, max_n_here, shared_stream ? 1 : count, persistent && !shared_stream,
+                       s, err, errlen);
+    if (rc) return rc;
+    if (shared_stream) {
+        s.grid = 1;
+        s.warps_per_cta = 1;
+    }
+    if (max_n_here > s.cap_n) {
+        rc = ensure_scratch(P, (int64_t)s.grid * s.warps_per_cta, max_n_here, err, errlen);
+        if (rc) return rc;
+    }
+    a.items = items;
+    a.num_items = count;
+    a.smem_cap_n = s.cap_n;
+    a.scratch_de = P->scratch_de.ptr;
+    a.scratch_s = P->scratch_s.ptr;
+    a.scratch_stride = P->scratch_stride;
+    a.num_slots = P->scratch_slots;
+    if (persistent && !shared_stream) {
+        B200SA_CUDA(cudaMemsetAsync(P->qhead.ptr, 0, sizeof(unsigned long long), st));
+        a.queue_head = P->qhead.ptr;
+    }
+    B200SA_CUDA(launch_sa(a, s.grid, s.warps_per_cta, s.region, st));
+    return B200SA_OK;
+}
+
+int collect_stats(b200sa_plan_s *P, const std::vector<std::pair<int, int>> &ranges,
+                  b200sa_stats *stats, char *err, size_t errlen) {
+    // ranges: (problem, reads completed from read 0)
+    if (!stats) return B200SA_OK;
+    std::vector<ReadStats> hs((size_t)P->total_reads);
+    if (P->total_reads)
+        B200SA_CUDA(cudaMemcpy(hs.data(), P->dstats.ptr,
+                               sizeof(ReadStats) * (size_t)P->total_reads,
+                               cudaMemcpyDeviceToHost));
+    for (auto &pr : ranges) {
+        const int p = pr.first;
+        const int64_t att_per_read =
+            (int64_t)P->n[p] * P->sweeps[p];  // sweeps = sweeps_per_beta * num_betas
+        for (int r = 0; r < pr.second; ++r) {
+            const ReadStats &x = hs[(size_t)(P->read_off[p] + r)];
+            stats->flips += (int64_t)x.flips;
+            stats->passes += (int64_t)x.passes;
+            stats->near_ties += (int64_t)x.near_ties;
+            stats->attempts += att_per_read;
+            stats->reads += 1;
+        }
+    }
+    return B200SA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *b200sa_version(void) { return "b200sa 0.1.0 (sm_100a)"; }
+
+int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
+                       int32_t device, b200sa_plan *out, char *err, size_t errlen) {
+    if (!out) return set_err(err, errlen, B200SA_EINVAL, "out is NULL");
+    *out = nullptr;
+    if (num_problems < 0 || (num_problems > 0 && !problems))
+        return set_err(err, errlen, B200SA_EINVAL, "bad problem list");
+    for (int32_t i = 0; i < num_problems; ++i) {
+        std::string msg;
+        const int rc = validate_problem(problems[i], msg);
+        if (rc) return set_err(err, errlen, rc, "problem " + std::to_string(i) + ": " + msg);
+        if (problems[i].num_reads > 0 && problems[i].num_vars > 0 && !problems[i].seeds)
+            return set_err(err, errlen, B200SA_EINVAL,
+                           "problem " + std::to_string(i) + ": seeds is NULL");
+    }
+    DeviceGuard guard;
+    std::unique_ptr<b200sa_plan_s> P(new b200sa_plan_s());
+    int rc = select_device(device, P->prop, err, errlen);
+    if (rc) return rc;
+    P->device = device;
+    B200SA_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+    B200SA_CUDA(cudaEventCreate(&P->ev0));
+    B200SA_CUDA(cudaEventCreate(&P->ev1));
+    P->num_problems = num_problems;
+
+    // Pack and lay out every problem in one device arena.
+    std::vector<PackedAdjacency> adj((size_t)num_problems);
+    struct Off {
+        size_t row, col, w, h, vinfo, cu, cv, cw, betas, thr;
+    };
+    std::vector<Off> off((size_t)num_problems);
+    size_t bytes = 0;
+    auto take = [&](size_t sz) {
+        const size_t o = bytes;
+        bytes = align16(bytes + sz);
+        return o;
+    };
+    P->state_off.assign((size_t)num_problems + 1, 0);
+    P->read_off.assign((size_t)num_problems + 1, 0);
+    for (int32_t i = 0; i < num_problems; ++i) {
+        const b200sa_problem &q = problems[i];
+        pack_adjacency(q, adj[i]);
+        const size_t n = (size_t)q.num_vars, m = (size_t)q.num_couplers,
+                     nb = (size_t)q.num_betas;
+        Off &o = off[i];
+        o.row = take(4 * (n + 1));
+        o.col = take(4 * 2 * m);
+        o.w = take(8 * 2 * m);
+        o.h = take(8 * n);
+        o.vinfo = take(n);
+        o.cu = take(4 * m);
+        o.cv = take(4 * m);
+        o.cw = take(8 * m);
+        o.betas = take(8 * nb);
+        o.thr = take(8 * nb);
+        P->state_off[i + 1] = P->state_off[i] + (int64_t)q.num_reads * q.num_vars;
+        P->read_off[i + 1] = P->read_off[i] + q.num_reads;
+        P->n.push_back(q.num_vars);
+        P->reads.push_back(q.num_reads);
+        P->sweeps.push_back(q.sweeps_per_beta * q.num_betas);
+        P->max_n = std::max(P->max_n, q.num_vars);
+    }
+    P->total_state = P->state_off[num_problems];
+    P->total_reads = P->read_off[num_problems];
+    std::vector<uint8_t> staging(bytes);
+    for (int32_t i = 0; i < num_problems; ++i) {
+        const b200sa_problem &q = problems[i];
+        const Off &o = off[i];
+        const size_t n = (size_t)q.num_vars, m = (size_t)q.num_couplers,
+                     nb = (size_t)q.num_betas;
+        std::memcpy(&staging[o.row], adj[i].row.data(), 4 * (n + 1));
+        if (m) {
+            std::memcpy(&staging[o.col], adj[i].col.data(), 4 * 2 * m);
+            std::memcpy(&staging[o.w], adj[i].w.data(), 8 * 2 * m);
+            std::memcpy(&staging[o.cu], q.coupler_starts, 4 * m);
+            std::memcpy(&staging[o.cv], q.coupler_ends, 4 * m);
+            std::memcpy(&staging[o.cw], q.coupler_weights, 8 * m);
+        }
+        if (n) {
+            std::memcpy(&staging[o.h], q.h, 8 * n);
+            std::memcpy(&staging[o.vinfo], adj[i].vinfo.data(), n);
+        }
+        if (nb) {
+            std::memcpy(&staging[o.betas], q.beta_schedule, 8 * nb);
+            double *thr = reinterpret_cast<double *>(&staging[o.thr]);
+            // cpu_sa.cpp:131, evaluated once per beta on the host (IEEE division).
+            for (size_t b = 0; b < nb; ++b) thr[b] = 44.36142 / q.beta_schedule[b];
+        }
+    }
+    B200SA_CUDA(P->arena.alloc(std::max<size_t>(bytes, 16)));
+    if (bytes)
+        B200SA_CUDA(cudaMemcpyAsync(P->arena.ptr, staging.data(), bytes,
+                                    cudaMemcpyHostToDevice, P->stream));
+    P->hprobs.resize((size_t)num_problems);
+    for (int32_t i = 0; i < num_problems; ++i) {
+        const b200sa_problem &q = problems[i];
+        const Off &o = off[i];
+        ProblemDev &d = P->hprobs[i];
+        uint8_t *base = P->arena.ptr;
+        d.n = q.num_vars;
+        d.sweeps_per_beta = q.sweeps_per_beta;
+        d.num_betas = q.num_betas;
+        d.num_reads = q.num_reads;
+        d.m = q.num_couplers;
+        d.state_offset = P->state_off[i];
+        d.read_offset = P->read_off[i];
+        d.row = reinterpret_cast<const int32_t *>(base + o.row);
+        d.col = reinterpret_cast<const int32_t *>(base + o.col);
+        d.w = reinterpret_cast<const double *>(base + o.w);
+        d.h = reinterpret_cast<const double *>(base + o.h);
+        d.vinfo = base + o.vinfo;
+        d.cu = reinterpret_cast<const int32_t *>(base + o.cu);
+        d.cv = reinterpret_cast<const int32_t *>(base + o.cv);
+        d.cw = reinterpret_cast<const double *>(base + o.cw);
+        d.betas = reinterpret_cast<const double *>(base + o.betas);
+        d.thresholds = reinterpret_cast<const double *>(base + o.thr);
+        d.varorder = q.varorder;
+        d.proposal = q.proposal;
+    }
+    B200SA_CUDA(P->dprobs.alloc((size_t)std::max(num_problems, 1)));
+    if (num_problems)
+        B200SA_CUDA(cudaMemcpyAsync(P->dprobs.ptr, P->hprobs.data(),
+                                    sizeof(ProblemDev) * (size_t)num_problems,
+                                    cudaMemcpyHostToDevice, P->stream));
+
+    // Seeds and work items.
+    std::vector<uint64_t> seeds((size_t)P->total_reads);
+    std::vector<int64_t> plain, lpt;
+    plain.reserve((size_t)P->total_reads);
+    P->plain_item_off.assign((size_t)num_problems + 1, 0);
+    for (int32_t i = 0; i < num_problems; ++i) {
+        const b200sa_problem &q = problems[i];
+        P->plain_item_off[i] = (int64_t)plain.size();
+        if (q.num_vars == 0) continue;  // nothing to anneal; energies are zero
+        for (int32_t r = 0; r < q.num_reads; ++r) {
+            seeds[(size_t)(P->read_off[i] + r)] = q.seeds[r];
+            plain.push_back(((int64_t)i << 32) | (int64_t)r);
+        }
+    }
+    P->plain_item_off[num_problems] = (int64_t)plain.size();
+    lpt = plain;
+    // Longest work first so the tail of a persistent launch is short.
+    std::stable_sort(lpt.begin(), lpt.end(), [&](int64_t a, int64_t b) {
+        const int pa = (int)(a >> 32), pb = (int)(b >> 32);
+        const int64_t ca = (int64_t)P->n[pa] * P->sweeps[pa];
+        const int64_t cb = (int64_t)P->n[pb] * P->sweeps[pb];
+        return ca > cb;
+    });
+    B200SA_CUDA(P->dseeds.alloc(std::max<size_t>(seeds.size(), 1)));
+    B200SA_CUDA(P->dstats.alloc(std::max<size_t>(seeds.size(), 1)));
+    B200SA_CUDA(P->items_plain.alloc(std::max<size_t>(plain.size(), 1)));
+    B200SA_CUDA(P->items_lpt.alloc(std::max<size_t>(lpt.size(), 1)));
+    B200SA_CUDA(P->qhead.alloc(1));
+    if (!seeds.empty())
+        B200SA_CUDA(cudaMemcpyAsync(P->dseeds.ptr, seeds.data(), 8 * seeds.size(),
+                                    cudaMemcpyHostToDevice, P->stream));
+    if (!plain.empty()) {
+        B200SA_CUDA(cudaMemcpyAsync(P->items_plain.ptr, plain.data(), 8 * plain.size(),
+                                    cudaMemcpyHostToDevice, P->stream));
+        B200SA_CUDA(cudaMemcpyAsync(P->items_lpt.ptr, lpt.data(), 8 * lpt.size(),
+                                    cudaMemcpyHostToDevice, P->stream));
+    }
+    B200SA_CUDA(upload_jump_columns(jump_columns(), P->stream));
+    B200SA_CUDA(cudaStreamSynchronize(P->stream));
+    *out = P.release();
+    return B200SA_OK;
+}
+
+int b200sa_plan_layout(b200sa_plan plan, int64_t *state_offsets, int64_t *read_offsets) {
+    if (!plan) return B200SA_EINVAL;
+    for (int i = 0; i <= plan->num_problems; ++i) {
+        if (state_offsets) state_offsets[i] = plan->state_off[i];
+        if (read_offsets) read_offsets[i] = plan->read_off[i];
+    }
+    return B200SA_OK;
+}
+
+int b200sa_plan_destroy(b200sa_plan plan) {
+    if (!plan) return B200SA_OK;
+    DeviceGuard guard;
+    cudaSetDevice(plan->device);
+    cudaStreamSynchronize(plan->stream);
+    delete plan;
+    return B200SA_OK;
+}
+
+int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
+                    int8_t *d_states_out, double *d_energies, const uint64_t *d_seeds,
+                    void *stream, int32_t sync, b200sa_stats *stats, char *err,
+                    size_t errlen) {
+    if (!plan) return set_err(err, errlen, B200SA_EINVAL, "plan is NULL");
+    if (mode != B200SA_MODE_PERSISTENT && mode != B200SA_MODE_PLAIN)
+        return set_err(err, errlen, B200SA_EINVAL, "unknown mode");
+    if (plan->total_reads > 0 && (!d_states_in || !d_states_out || !d_energies))
+        return set_err(err, errlen, B200SA_EINVAL, "device buffers are NULL");
+    DeviceGuard guard;
+    B200SA_CUDA(cudaSetDevice(plan->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    LaunchArgs a = base_args(plan, d_states_in, d_states_out, d_energies, d_seeds);
+    // Problems with no variables: energies are 0 (cpu_sa.cpp:217-226 over nothing).
+    for (int i = 0; i < plan->num_problems; ++i) {
+        if (plan->n[i] == 0 && plan->reads[i] > 0)
+            B200SA_CUDA(cudaMemsetAsync(d_energies + plan->read_off[i], 0,
+                                        sizeof(double) * (size_t)plan->reads[i], st));
+    }
+    B200SA_CUDA(cudaEventRecord(plan->ev0, st));
+    int rc = B200SA_OK;
+    if (mode == B200SA_MODE_PERSISTENT) {
+        rc = launch_items(plan, a, plan->items_lpt.ptr,
+                          plan->plain_item_off[plan->num_problems], plan->max_n, true,
+                          false, st, err, errlen);
+    } else {
+        for (int i = 0; i < plan->num_problems && rc == B200SA_OK; ++i) {
+            const int64_t o = plan->plain_item_off[i];
+            rc = launch_items(plan, a, plan->items_plain.ptr + o,
+                              plan->plain_item_off[i + 1] - o, plan->n[i], false, false,
+                              st, err, errlen);
+        }
+    }
+    if (rc) return rc;
+    B200SA_CUDA(cudaEventRecord(plan->ev1, st));
+    if (sync) {
+        B200SA_CUDA(cudaStreamSynchronize(st));
+        if (stats) {
+            float ms = 0.f;
+            B200SA_CUDA(cudaEventElapsedTime(&ms, plan->ev0, plan->ev1));
+            std::vector<std::pair<int, int>> ranges;
+            for (int i = 0; i < plan->num_problems; ++i)
+                ranges.emplace_back(i, plan->n[i] ? plan->reads[i] : 0);
+            rc = collect_stats(plan, ranges, stats, err, errlen);
+            if (rc) return rc;
+            for (int i = 0; i < plan->num_problems; ++i)
+                if (plan->n[i] == 0) stats->reads += plan->reads[i];
+            stats->kernel_ms = ms;
+        }
+    }
+    return B200SA_OK;
+}
+
+int b200sa_sample_batch(const b200sa_problem *problems, int32_t num_problems, int32_t mode,
+                        int32_t device, b200sa_stats *stats, char *err, size_t errlen) {
+    b200sa_plan plan = nullptr;
+    int rc = b200sa_plan_create(problems, num_problems, device, &plan, err, errlen);
+    if (rc) return rc;
+    std::unique_ptr<b200sa_plan_s, int (*)(b200sa_plan)> hold(plan, b200sa_plan_destroy);
+    DeviceGuard guard;
+    B200SA_CUDA(cudaSetDevice(plan->device));
+    DevArray<int8_t> dstates;
+    DevArray<double> den;
+    B200SA_CUDA(dstates.alloc((size_t)std::max<int64_t>(plan->total_state, 1)));
+    B200SA_CUDA(den.alloc((size_t)std::max<int64_t>(plan->total_reads, 1)));
+    for (int i = 0; i < num_problems; ++i) {
+        const size_t sz = (size_t)problems[i].num_reads * (size_t)problems[i].num_vars;
+        if (sz) {
+            if (!problems[i].states)
+                return set_err(err, errlen, B200SA_EINVAL,
+                               "problem " + std::to_string(i) + ": states is NULL");
+            B200SA_CUDA(cudaMemcpyAsync(dstates.ptr + plan->state_off[i], problems[i].states,
+                                        sz, cudaMemcpyHostToDevice, plan->stream));
+        }
+        if (problems[i].num_reads > 0 && !problems[i].energies)
+            return set_err(err, errlen, B200SA_EINVAL,
+                           "problem " + std::to_string(i) + ": energies is NULL");
+    }
+    rc = b200sa_plan_run(plan, mode, dstates.ptr, dstates.ptr, den.ptr, nullptr, nullptr, 1,
+                         stats, err, errlen);
+    if (rc) return rc;
+    for (int i = 0; i < num_problems; ++i) {
+        const size_t sz = (size_t)problems[i].num_reads * (size_t)problems[i].num_vars;
+        if (sz)
+            B200SA_CUDA(cudaMemcpyAsync(problems[i].states, dstates.ptr + plan->state_off[i],
+                                        sz, cudaMemcpyDeviceToHost, plan->stream));
+        if (problems[i].num_reads)
+            B200SA_CUDA(cudaMemcpyAsync(problems[i].energies, den.ptr + plan->read_off[i],
+                                        sizeof(double) * (size_t)problems[i].num_reads,
+                                        cudaMemcpyDeviceToHost, plan->stream));
+    }
+    B200SA_CUDA(cudaStreamSynchronize(plan->stream));
+    return (int)std::min<int64_t>(plan->total_reads, INT32_MAX);
+}
+
+int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
+                  const int32_t *coupler_starts, const int32_t *coupler_ends,
+                  const double *coupler_weights, int32_t num_reads, int8_t *states,
+                  double *energies, int32_t sweeps_per_beta, int32_t num_betas,
+                  const double *beta_schedule, const uint64_t *seeds, int32_t num_seeds,
+                  int32_t varorder, int32_t proposal, b200sa_interrupt_fn interrupt_fn,
+                  void *interrupt_ctx, int32_t device, b200sa_stats *stats, char *err,
+                  size_t errlen) {
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (num_reads < 0) return set_err(err, errlen, B200SA_EINVAL, "num_reads < 0");
+    if (num_reads == 0) return 0;
+    if (!states && num_vars > 0)
+        return set_err(err, errlen, B200SA_EINVAL, "states is NULL");
+    if (!energies) return set_err(err, errlen, B200SA_EINVAL, "energies is NULL");
+    if (!seeds || (num_seeds != 1 && num_seeds != num_reads))
+        return set_err(err, errlen, B200SA_EINVAL,
+                       "num_seeds must be 1 (one continued stream) or num_reads (per read)");
+    const bool shared = num_seeds == 1 && num_reads > 1;
+    std::vector<uint64_t> per_read;
+    if (num_seeds == 1 && !shared) per_read.assign(1, seeds[0]);
+    b200sa_problem q{};
+    q.num_vars = num_vars;
+    q.h = h;
+    q.num_couplers = num_couplers;
+    q.coupler_starts = coupler_starts;
+    q.coupler_ends = coupler_ends;
+    q.coupler_weights = coupler_weights;
+    q.num_reads = num_reads;
+    q.states = states;
+    q.energies = energies;
+    q.sweeps_per_beta = sweeps_per_beta;
+    q.num_betas = num_betas;
+    q.beta_schedule = beta_schedule;
+    std::vector<uint64_t> shared_seeds;
+    if (shared) {  // the kernel seeds only the first read and continues the stream
+        shared_seeds.assign((size_t)num_reads, seeds[0]);
+        q.seeds = shared_seeds.data();
+    } else {
+        q.seeds = per_read.empty() ? seeds : per_read.data();
+    }
+    q.varorder = varorder;
+    q.proposal = proposal;
+    if (num_vars == 0) {  // cpu_sa.cpp: every read's energy sums nothing
+        std::string msg;
+        int rc = validate_problem(q, msg);
+        if (rc) return set_err(err, errlen, rc, msg);
+        for (int32_t r = 0; r < num_reads; ++r) {
+            energies[r] = 0.0;
+            if (interrupt_fn && interrupt_fn(interrupt_ctx)) {
+                if (stats) stats->reads = r + 1;
+                return r + 1;
+            }
+        }
+        if (stats) stats->reads = num_reads;
+        return num_reads;
+    }
+    b200sa_plan plan = nullptr;
+    int rc = b200sa_plan_create(&q, 1, device, &plan, err, errlen);
+    if (rc) return rc;
+    std::unique_ptr<b200sa_plan_s, int (*)(b200sa_plan)> hold(plan, b200sa_plan_destroy);
+    DeviceGuard guard;
+    B200SA_CUDA(cudaSetDevice(plan->device));
+    const size_t n = (size_t)num_vars;
+    DevArray<int8_t> dstates;
+    DevArray<double> den;
+    B200SA_CUDA(dstates.alloc(n * (size_t)num_reads));
+    B200SA_CUDA(den.alloc((size_t)num_reads));
+    B200SA_CUDA(cudaMemcpyAsync(dstates.ptr, states, n * (size_t)num_reads,
+                                cudaMemcpyHostToDevice, plan->stream));
+    if (shared) B200SA_CUDA(plan->carry.alloc(kCarryWords));
+
+    // Chunks: everything at once without an interrupt; with one, a resident
+    // wave of reads (per-read seeds) or one read (continued stream) per launch,
+    // polling the callback after each completed read in read order.
+    int64_t chunk = num_reads;
+    if (interrupt_fn) {
+        if (shared) {
+            chunk = 1;
+        } else {
+            LaunchShape s{};
+            rc = shape_for(plan, num_vars, num_reads, true, s, err, errlen);
+            if (rc) return rc;
+            int per_sm = 0;
+            B200SA_CUDA(kernel_occupancy(s.warps_per_cta, s.region, &per_sm));
+            chunk = std::max<int64_t>(
+                1, (int64_t)plan->prop.multiProcessorCount * per_sm * s.warps_per_cta);
+        }
+    }
+    LaunchArgs a = base_args(plan, dstates.ptr, dstates.ptr, den.ptr, nullptr);
+    a.rng_carry = plan->carry.ptr;
+    a.shared_stream = shared ? 1 : 0;
+    float total_ms = 0.f;
+    int32_t done = 0;
+    bool stop = false;
+    while (done < num_reads && !stop) {
+        const int64_t cnt = std::min<int64_t>(chunk, num_reads - done);
+        a.carry_in = (shared && done > 0) ? 1 : 0;
+        B200SA_CUDA(cudaEventRecord(plan->ev0, plan->stream));
+        rc = launch_items(plan, a, plan->items_plain.ptr + done, cnt, num_vars, !shared,
+                          shared, plan->stream, err, errlen);
+        if (rc) return rc;
+        B200SA_CUDA(cudaEventRecord(plan->ev1, plan->stream));
+        B200SA_CUDA(cudaStreamSynchronize(plan->stream));
+        float ms = 0.f;
+        B200SA_CUDA(cudaEventElapsedTime(&ms, plan->ev0, plan->ev1));
+        total_ms += ms;
+        int32_t k = 0;
+        for (; k < cnt; ++k) {
+            if (interrupt_fn && interrupt_fn(interrupt_ctx)) {  // cpu_sa.cpp:357
+                stop = true;
+                ++k;
+                break;
+            }
+        }
+        // Only completed-and-kept reads are written back; later rows keep
+        // their initial states, as in the reference.
+        B200SA_CUDA(cudaMemcpyAsync(states + n * (size_t)done, dstates.ptr + n * (size_t)done,
+                                    n * (size_t)k, cudaMemcpyDeviceToHost, plan->stream));
+        B200SA_CUDA(cudaMemcpyAsync(energies + done, den.ptr + done, sizeof(double) * (size_t)k,
+                                    cudaMemcpyDeviceToHost, plan->stream));
+        B200SA_CUDA(cudaStreamSynchronize(plan->stream));
+        done += k;
+    }
+    if (stats) {
+        rc = collect_stats(plan, {{0, done}}, stats, err, errlen);
+        if (rc) return rc;
+        stats->kernel_ms = total_ms;
+    }
+    return done;
+}
+
+}  // extern "C"

@@ -1,0 +1,154 @@
+/*
+ * b200sa: B200 (sm_100a) simulated-annealing sampler -- C ABI.
+ *
+ * Drop-in for the simulated-annealing path of dwave-samplers 1.8.0:
+ *   C++ core   general_simulated_annealing   dwave/samplers/sa/src/cpu_sa.h:63-78
+ *                                             dwave/samplers/sa/src/cpu_sa.cpp:253-362
+ *   Cython     simulated_annealing(...)       dwave/samplers/sa/simulated_annealing.pyx:45-50
+ *
+ * Conventions shared by every entry point
+ *   - Plain C types only; no exceptions cross this boundary.  Every function
+ *     returns a non-negative value on success and a negative B200SA_E* code on
+ *     failure, with a message in `err` (NUL-terminated, truncated to errlen)
+ *     when `err` is non-NULL.  The reference throws std::runtime_error through
+ *     a nogil Cython call for the same conditions (cpu_sa.cpp:276-279,
+ *     302-304), which aborts the process.
+ *   - States are int8 spins, row-major num_reads x num_vars, C-contiguous.
+ *   - Enumerations keep the reference's numeric values (cpu_sa.h:36-43).
+ *   - Seeding.  With num_seeds == num_reads, read r uses its own xorshift128+
+ *     stream seeded with seeds[r] and equals a reference call with
+ *     num_samples=1, seed=seeds[r].  With num_seeds == 1 the stream is seeded
+ *     once and continues across reads exactly as in the reference
+ *     (cpu_sa.cpp:283-284, 321-358); that mode runs the reads one after
+ *     another on one warp.
+ *   - Reentrant: no global mutable state; each call uses its own stream and
+ *     device buffers.
+ */
+#ifndef B200SA_H
+#define B200SA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define B200SA_API __attribute__((visibility("default")))
+#else
+#define B200SA_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200SA_OK 0
+#define B200SA_EINVAL (-1)   /* bad argument: lengths, indices, enums */
+#define B200SA_ECUDA (-2)    /* CUDA runtime error (message has the detail) */
+#define B200SA_ENOMEM (-3)   /* host or device allocation failed */
+#define B200SA_ENODEV (-4)   /* no usable sm_100 device */
+#define B200SA_ETIMEOUT (-5) /* a bounded device wait expired */
+
+/* cpu_sa.h:36-39 */
+#define B200SA_GIBBS 0
+#define B200SA_METROPOLIS 1
+/* cpu_sa.h:40-43 */
+#define B200SA_SEQUENTIAL 0
+#define B200SA_RANDOM 1
+
+/* Scheduling modes for the batched entry points. */
+#define B200SA_MODE_PERSISTENT 0 /* one launch, device work queue over (problem, read) */
+#define B200SA_MODE_PLAIN 1      /* one launch per problem, problems in order */
+
+/* Replaces the reference's `callback` (cpu_sa.h:61): called between reads,
+ * in read order, for each completed read; nonzero stops sampling and the
+ * completed prefix is returned (cpu_sa.cpp:357). */
+typedef int (*b200sa_interrupt_fn)(void *ctx);
+
+typedef struct {
+    int64_t reads;        /* reads completed */
+    int64_t attempts;     /* spin-flip attempts: reads x sweeps x num_vars */
+    int64_t flips;        /* accepted flips */
+    int64_t near_ties;    /* exp() decisions inside the cross-libm tie band */
+    int64_t passes;       /* warp passes of the sequential sweep (speculation efficiency) */
+    double kernel_ms;     /* device time of the sampling launches (CUDA events) */
+} b200sa_stats;
+
+/* One binary quadratic model in Ising form plus its reads.
+ * Couplers are COO in input order; that order fixes the adjacency order and
+ * the energy summation order exactly as in cpu_sa.cpp:298-316 and :210-227. */
+typedef struct {
+    int32_t num_vars;
+    const double *h;                /* [num_vars] */
+    int64_t num_couplers;
+    const int32_t *coupler_starts;  /* [num_couplers] */
+    const int32_t *coupler_ends;    /* [num_couplers] */
+    const double *coupler_weights;  /* [num_couplers] */
+    int32_t num_reads;
+    int8_t *states;                 /* [num_reads * num_vars], in/out */
+    double *energies;               /* [num_reads], out */
+    int32_t sweeps_per_beta;
+    int32_t num_betas;
+    const double *beta_schedule;    /* [num_betas] */
+    const uint64_t *seeds;          /* [num_reads] per-read seeds */
+    int32_t varorder;               /* B200SA_SEQUENTIAL / B200SA_RANDOM */
+    int32_t proposal;               /* B200SA_GIBBS / B200SA_METROPOLIS */
+} b200sa_problem;
+
+/* Replaces general_simulated_annealing (cpu_sa.h:63-78, cpu_sa.cpp:253-362)
+ * behind simulated_annealing.pyx:172-186.  Host buffers; `states` is
+ * overwritten in place for the reads completed.  Returns the number of reads
+ * completed (num_reads unless interrupted) or a negative error. */
+B200SA_API int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
+                  const int32_t *coupler_starts, const int32_t *coupler_ends,
+                  const double *coupler_weights, int32_t num_reads,
+                  int8_t *states, double *energies, int32_t sweeps_per_beta,
+                  int32_t num_betas, const double *beta_schedule,
+                  const uint64_t *seeds, int32_t num_seeds, int32_t varorder,
+                  int32_t proposal, b200sa_interrupt_fn interrupt_fn,
+                  void *interrupt_ctx, int32_t device, b200sa_stats *stats,
+                  char *err, size_t errlen);
+
+/* Many independent problems (uneven sizes, read counts and schedules), host
+ * buffers.  The reference has no batched entry point; each problem's reads
+ * equal the per-read reference calls.  mode: B200SA_MODE_*.
+ * Returns the total number of reads completed or a negative error. */
+B200SA_API int b200sa_sample_batch(const b200sa_problem *problems, int32_t num_problems,
+                        int32_t mode, int32_t device, b200sa_stats *stats,
+                        char *err, size_t errlen);
+
+/* ---- Device-resident plans (inputs kept in HBM across runs) --------------
+ * A plan packs the problems (order-preserving CSR, schedules, seeds) once and
+ * keeps them on the device.  Runs take DEVICE pointers for the states, laid
+ * out problem after problem (see b200sa_plan_layout).  No reference
+ * counterpart: this is the resident form of b200sa_sample_batch. */
+typedef struct b200sa_plan_s *b200sa_plan;
+
+B200SA_API int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
+                       int32_t device, b200sa_plan *out, char *err,
+                       size_t errlen);
+
+/* Per-problem element offsets into the concatenated state array (int8) and
+ * read offsets into the energy / seed arrays; each array has num_problems+1
+ * entries (the last is the total). */
+B200SA_API int b200sa_plan_layout(b200sa_plan plan, int64_t *state_offsets,
+                       int64_t *read_offsets);
+
+/* Anneal on the device.  d_states_in may equal d_states_out.  d_seeds may be
+ * NULL (the seeds given at plan creation are used).  `stream` is a
+ * cudaStream_t (NULL = the plan's own stream).  The call returns after the
+ * work is enqueued when `sync` is 0, and after it completes when 1 (stats
+ * are filled only when sync is 1). */
+B200SA_API int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
+                    int8_t *d_states_out, double *d_energies,
+                    const uint64_t *d_seeds, void *stream, int32_t sync,
+                    b200sa_stats *stats, char *err, size_t errlen);
+
+B200SA_API int b200sa_plan_destroy(b200sa_plan plan);
+
+/* Version string of this library. */
+B200SA_API const char *b200sa_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200SA_H */

@@ -1,0 +1,41 @@
+#!/usr/bin/env bash
+# Build the reference's own simulated-annealing extension from its sources, for
+# use as a test oracle and as the timed CPU baseline.  Test infrastructure only.
+#
+# Sources (read in place, never copied into the repository):
+#   <ref>/dwave/samplers/sa/simulated_annealing.pyx   (Cython binding)
+#   <ref>/dwave/samplers/sa/src/cpu_sa.cpp, cpu_sa.h   (C++ core)
+# Flags follow the reference's meson.build:4-12,22 (C++17, -O3, release
+# => -DNDEBUG, -g1; no -march, no fast-math).
+#
+# Output: oracle/_ref/simulated_annealing<EXT_SUFFIX> (git-ignored; it travels
+# with the working tree to machines that do not have the reference sources).
+set -euo pipefail
+
+REF="${1:-/root/reference}"
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+OUT="$HERE/_ref"
+SA="$REF/dwave/samplers/sa"
+
+if [ ! -f "$SA/simulated_annealing.pyx" ]; then
+    echo "reference sources not found under $REF; skipping" >&2
+    exit 0
+fi
+
+mkdir -p "$OUT"
+PY="${PYTHON:-python}"
+EXT_SUFFIX="$($PY -c 'import sysconfig; print(sysconfig.get_config_var("EXT_SUFFIX"))')"
+PYINC="$($PY -c 'import sysconfig; print(sysconfig.get_paths()["include"])')"
+NPINC="$($PY -c 'import numpy; print(numpy.get_include())')"
+
+# Cython writes the generated C++ next to the requested output path.
+$PY -m cython --cplus -3 -Xfreethreading_compatible=True \
+    -o "$OUT/simulated_annealing.cpp" "$SA/simulated_annealing.pyx"
+
+g++ -O3 -std=c++17 -g1 -DNDEBUG -fPIC -shared -Wall -Wno-unused-function \
+    -I"$SA/src" -I"$PYINC" -I"$NPINC" \
+    "$OUT/simulated_annealing.cpp" "$SA/src/cpu_sa.cpp" \
+    -o "$OUT/simulated_annealing$EXT_SUFFIX"
+
+rm -f "$OUT/simulated_annealing.cpp"
+echo "built $OUT/simulated_annealing$EXT_SUFFIX"

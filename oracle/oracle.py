@@ -1,0 +1,147 @@
+"""Python access to the CPU oracle.  TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
+``bench.py`` import this module; the product package never does.
+
+Two oracles are exposed:
+
+* :func:`run` -- the C restatement in ``oracle/sa_oracle.c`` of the
+  reference's ``general_simulated_annealing`` (dwave-samplers 1.8.0,
+  ``dwave/samplers/sa/src/cpu_sa.cpp:253-362``).
+* :func:`reference_module` -- the reference's own Cython extension
+  (``dwave/samplers/sa/simulated_annealing.pyx``) built from its sources by
+  ``oracle/build_ref.sh`` into ``oracle/_ref/``, when that build exists.
+"""
+from __future__ import annotations
+
+import ctypes
+import importlib.util
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(HERE, "libsa_oracle.so")
+_REF_DIR = os.path.join(HERE, "_ref")
+
+_lib = None
+_ref = None
+
+
+def build() -> str:
+    """Compile the C restatement (plain gcc) if it is missing or stale."""
+    src = os.path.join(HERE, "sa_oracle.c")
+    if (not os.path.exists(_LIB_PATH)
+            or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src)):
+        subprocess.check_call(["make", "-s", "-C", HERE, "libsa_oracle.so"])
+    return _LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.sa_oracle_run.restype = ctypes.c_int
+        L.sa_oracle_run.argtypes = [
+            ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.sa_oracle_energy.restype = ctypes.c_double
+        L.sa_oracle_energy.argtypes = [
+            ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.sa_oracle_rng_stream.restype = None
+        L.sa_oracle_rng_stream.argtypes = [ctypes.c_uint64, ctypes.c_int,
+                                           ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def run(h, u, v, J, states, sweeps_per_beta, betas, seeds,
+        randomize_order=False, gibbs=False):
+    """Anneal ``states`` (R x n int8, copied) with the C restatement.
+
+    ``seeds`` is either one seed (one stream continued across reads, the
+    reference's multi-read behaviour) or one seed per read (each read equal to
+    a reference call with ``num_samples=1, seed=seeds[r]``).
+    Returns ``(states, energies)``.
+    """
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.int32)
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    st = np.array(states, dtype=np.int8, order="C", copy=True)
+    if st.ndim != 2 or st.shape[1] != h.shape[0]:
+        raise ValueError("states must be (num_reads, num_vars)")
+    betas = np.ascontiguousarray(betas, dtype=np.float64)
+    seeds = np.atleast_1d(np.asarray(seeds, dtype=np.uint64))
+    R, n = st.shape
+    en = np.zeros(R, dtype=np.float64)
+    rc = lib().sa_oracle_run(
+        n, _ptr(h), len(J), _ptr(u), _ptr(v), _ptr(J), R, _ptr(st), _ptr(en),
+        int(sweeps_per_beta), len(betas), _ptr(betas), _ptr(seeds), len(seeds),
+        int(bool(randomize_order)), int(bool(gibbs)))
+    if rc < 0:
+        raise ValueError(f"oracle error {rc}")
+    return st, en
+
+
+def energy(h, u, v, J, state) -> float:
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.int32)
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    s = np.ascontiguousarray(state, dtype=np.int8)
+    return lib().sa_oracle_energy(len(h), _ptr(h), len(J), _ptr(u), _ptr(v),
+                                  _ptr(J), _ptr(s))
+
+
+def rng_stream(seed: int, count: int) -> np.ndarray:
+    out = np.zeros(count, dtype=np.uint64)
+    lib().sa_oracle_rng_stream(int(seed), int(count), _ptr(out))
+    return out
+
+
+def reference_module():
+    """The reference extension built from source, or None if not built."""
+    global _ref
+    if _ref is not None:
+        return _ref
+    if not os.path.isdir(_REF_DIR):
+        return None
+    for name in os.listdir(_REF_DIR):
+        if name.startswith("simulated_annealing") and name.endswith(".so"):
+            spec = importlib.util.spec_from_file_location(
+                "simulated_annealing", os.path.join(_REF_DIR, name))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            _ref = mod
+            return _ref
+    return None
+
+
+def reference_per_read(h, u, v, J, states, sweeps_per_beta, betas, seeds,
+                       randomize_order=False, proposal="Metropolis"):
+    """Run the reference extension once per read (num_samples=1, seed=seeds[r])."""
+    mod = reference_module()
+    if mod is None:
+        raise RuntimeError("reference extension not built (oracle/build_ref.sh)")
+    st = np.array(states, dtype=np.int8, order="C", copy=True)
+    en = np.zeros(st.shape[0])
+    hl, ul, vl, Jl = list(map(float, h)), list(map(int, u)), list(map(int, v)), list(map(float, J))
+    for r in range(st.shape[0]):
+        row = st[r:r + 1].copy()
+        s, e = mod.simulated_annealing(1, hl, ul, vl, Jl, int(sweeps_per_beta),
+                                       np.asarray(betas, dtype=float), int(seeds[r]), row,
+                                       randomize_order, proposal)
+        st[r] = s[0]
+        en[r] = e[0]
+    return st, en

@@ -1,0 +1,197 @@
+/*
+ * CPU restatement of the reference simulated-annealing sweep.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle for the CUDA
+ * sampler: only tests, the smoke check and the CPU-baseline leg of the
+ * benchmark load it.  The product library never links or calls it.
+ *
+ * It restates, in plain C, the algorithm of dwave-samplers 1.8.0
+ * (dwave/samplers/sa/src/cpu_sa.cpp); every function names the lines it
+ * follows.  It is pinned against the reference extension built from source
+ * (oracle/build_ref.sh) by tests/test_oracle.py and against the committed
+ * golden vectors in tests/golden/.
+ *
+ * Two seeding modes:
+ *   num_seeds == 1         : one xorshift128+ stream seeded once per call and
+ *                            continued across reads (cpu_sa.cpp:283-284, 321-358)
+ *   num_seeds == num_reads : read r is an independent call with num_samples=1
+ *                            and seed=seeds[r] (the per-read contract).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define ORACLE_EINVAL (-1)
+#define ORACLE_ENOMEM (-2)
+
+/* xorshift128+ step, cpu_sa.cpp:27-34.  Returns s1_new + s1_old. */
+static inline uint64_t rng_next(uint64_t st[2]) {
+    uint64_t a = st[0];
+    const uint64_t b = st[1];
+    st[0] = b;
+    a ^= a << 23;
+    st[1] = a ^ b ^ (a >> 17) ^ (b >> 26);
+    return st[1] + b;
+}
+
+/* Seeding, cpu_sa.cpp:283-284: zero is replaced by 2^64-1. */
+static inline void rng_seed(uint64_t st[2], uint64_t seed) {
+    st[0] = seed ? seed : UINT64_MAX;
+    st[1] = 0;
+}
+
+/* The reference's RANDMAX ((uint64_t)-1) used as a double operand rounds to
+ * 2^64 (cpu_sa.cpp:36, 154, 163). */
+static const double RANDMAX_D = 18446744073709551616.0;
+
+typedef struct {
+    int n;
+    int *row;     /* n+1 offsets */
+    int *col;     /* neighbour index, per adjacency entry */
+    double *w;    /* coupling, per adjacency entry */
+} adjacency;
+
+/* Adjacency in coupler input order, cpu_sa.cpp:298-316: coupler c appends v
+ * to u's list and u to v's list (a self-loop appends v twice to its own list).
+ * A counting sort over the coupler list reproduces the push_back order. */
+static int build_adjacency(adjacency *a, int n, long m, const int *u,
+                           const int *v, const double *J) {
+    a->n = n;
+    a->row = (int *)calloc((size_t)n + 1, sizeof(int));
+    a->col = (int *)malloc(sizeof(int) * (size_t)(2 * m + 1));
+    a->w = (double *)malloc(sizeof(double) * (size_t)(2 * m + 1));
+    int *cur = (int *)malloc(sizeof(int) * ((size_t)n + 1));
+    if (!a->row || !a->col || !a->w || !cur) {
+        free(cur);
+        return ORACLE_ENOMEM;
+    }
+    for (long c = 0; c < m; c++) {
+        if (u[c] < 0 || v[c] < 0 || u[c] >= n || v[c] >= n) {
+            free(cur);
+            return ORACLE_EINVAL; /* cpu_sa.cpp:302-304 throws here */
+        }
+        a->row[u[c] + 1]++;
+        a->row[v[c] + 1]++;
+    }
+    for (int i = 0; i < n; i++) a->row[i + 1] += a->row[i];
+    memcpy(cur, a->row, sizeof(int) * (size_t)n);
+    for (long c = 0; c < m; c++) {
+        int k = cur[u[c]]++;
+        a->col[k] = v[c];
+        a->w[k] = J[c];
+        k = cur[v[c]]++;
+        a->col[k] = u[c];
+        a->w[k] = J[c];
+    }
+    free(cur);
+    return 0;
+}
+
+static void free_adjacency(adjacency *a) {
+    free(a->row);
+    free(a->col);
+    free(a->w);
+}
+
+/* Energy change of flipping `var`, cpu_sa.cpp:54-74: the local field is
+ * summed left to right in adjacency order, then scaled by -2*s. */
+static double flip_energy(int var, const int8_t *s, const double *h,
+                          const adjacency *a) {
+    double f = h[var];
+    for (int k = a->row[var]; k < a->row[var + 1]; k++)
+        f += s[a->col[k]] * a->w[k];
+    return (-2 * s[var]) * f;
+}
+
+/* One read, cpu_sa.cpp:93-197.  `order` 0 = sequential, 1 = random;
+ * `gibbs` 0 = Metropolis, 1 = Gibbs. */
+static void anneal_one(int8_t *s, const double *h, const adjacency *a,
+                       int sweeps_per_beta, int num_betas, const double *betas,
+                       int order, int gibbs, uint64_t st[2], double *de) {
+    const int n = a->n;
+    for (int i = 0; i < n; i++) de[i] = flip_energy(i, s, h, a);
+
+    for (int b = 0; b < num_betas; b++) {
+        const double beta = betas[b];
+        for (int sw = 0; sw < sweeps_per_beta; sw++) {
+            const double threshold = 44.36142 / beta; /* cpu_sa.cpp:131 */
+            for (int i = 0; i < n; i++) {
+                int var = i;
+                if (order) var = (int)(rng_next(st) % (uint64_t)n); /* :134-136 */
+                if (de[var] >= threshold) continue;                 /* :140 */
+                int flip = 0;
+                if (!gibbs) { /* Metropolis, :144-158 */
+                    if (de[var] <= 0.0) {
+                        flip = 1;
+                    } else {
+                        uint64_t r = rng_next(st);
+                        if (exp(-de[var] * beta) * RANDMAX_D > (double)r) flip = 1;
+                    }
+                } else { /* Gibbs, :159-166 */
+                    uint64_t r = rng_next(st);
+                    if (RANDMAX_D > (double)r * (1 + exp(de[var] * beta))) flip = 1;
+                }
+                if (flip) { /* :168-191 */
+                    const int8_t mult = (int8_t)(4 * s[var]);
+                    for (int k = a->row[var]; k < a->row[var + 1]; k++) {
+                        const int nb = a->col[k];
+                        de[nb] += mult * a->w[k] * s[nb];
+                    }
+                    s[var] = (int8_t)(-s[var]);
+                    de[var] = -de[var];
+                }
+            }
+        }
+    }
+}
+
+/* State energy, cpu_sa.cpp:210-227: fields in variable order, then couplers
+ * in input order, one running double. */
+double sa_oracle_energy(int n, const double *h, long m, const int *u,
+                        const int *v, const double *J, const int8_t *s) {
+    double e = 0.0;
+    for (int i = 0; i < n; i++) e += s[i] * h[i];
+    for (long c = 0; c < m; c++) e += s[u[c]] * J[c] * s[v[c]];
+    return e;
+}
+
+/* Driver, cpu_sa.cpp:253-362.  Returns reads completed (no interrupt here:
+ * interrupt polling is host logic tested elsewhere) or a negative error. */
+int sa_oracle_run(int n, const double *h, long m, const int *u, const int *v,
+                  const double *J, int num_reads, int8_t *states,
+                  double *energies, int sweeps_per_beta, int num_betas,
+                  const double *betas, const uint64_t *seeds, int num_seeds,
+                  int order, int gibbs) {
+    if (num_reads < 0 || n < 0 || m < 0) return ORACLE_EINVAL;
+    if (num_seeds != 1 && num_seeds != num_reads) return ORACLE_EINVAL;
+    if (num_reads == 0 || n == 0) return num_reads;
+    adjacency a;
+    memset(&a, 0, sizeof(a));
+    int rc = build_adjacency(&a, n, m, u, v, J);
+    double *de = (double *)malloc(sizeof(double) * (size_t)n);
+    if (rc != 0 || !de) {
+        free_adjacency(&a);
+        free(de);
+        return rc ? rc : ORACLE_ENOMEM;
+    }
+    uint64_t st[2] = {0, 0};
+    if (num_seeds == 1) rng_seed(st, seeds[0]);
+    for (int r = 0; r < num_reads; r++) {
+        if (num_seeds != 1) rng_seed(st, seeds[r]);
+        int8_t *s = states + (size_t)r * (size_t)n;
+        anneal_one(s, h, &a, sweeps_per_beta, num_betas, betas, order, gibbs,
+                   st, de);
+        energies[r] = sa_oracle_energy(n, h, m, u, v, J, s);
+    }
+    free(de);
+    free_adjacency(&a);
+    return num_reads;
+}
+
+/* First `count` xorshift128+ outputs for `seed` (used by RNG unit tests). */
+void sa_oracle_rng_stream(uint64_t seed, int count, uint64_t *out) {
+    uint64_t st[2];
+    rng_seed(st, seed);
+    for (int i = 0; i < count; i++) out[i] = rng_next(st);
+}

@@ -1,0 +1,321 @@
+"""CUDA path vs the reference: golden vectors, the oracle, and the reference's
+own Cython-level tests (tests/test_simulated_annealing.py) restated.
+
+Bit-exact bar: states equal and energies equal bit for bit; the kernel's
+near-tie counter (exp decisions within 2^-48 relative of the threshold, where
+CUDA's exp and the host libm could disagree) must be zero.
+"""
+import threading
+
+import numpy as np
+import pytest
+
+import oracle
+from b200sa import Plan, sample_batch, simulated_annealing
+from b200sa import workloads
+from conftest import GOLDEN, bits, load_golden
+
+pytestmark = pytest.mark.gpu
+
+CRIT = {0: "Gibbs", 1: "Metropolis"}
+
+
+def run_cuda(c, **kw):
+    st = np.array(c["states0"], dtype=np.int8, copy=True)
+    R = st.shape[0]
+    stats = {}
+    if bool(c["shared"]):
+        s, e = simulated_annealing(R, c["h"], c["u"], c["v"], c["J"], int(c["spb"]), c["betas"],
+                                   int(c["seeds"][0]), st, bool(c["order"]),
+                                   CRIT[int(c["proposal"])], rng_stream="shared", stats=stats, **kw)
+    else:
+        s, e = simulated_annealing(R, c["h"], c["u"], c["v"], c["J"], int(c["spb"]), c["betas"],
+                                   0, st, bool(c["order"]), CRIT[int(c["proposal"])],
+                                   seeds=c["seeds"], stats=stats, **kw)
+    return s, e, stats
+
+
+@pytest.mark.parametrize("name", GOLDEN)
+def test_golden_vectors(name):
+    c = load_golden(name)
+    s, e, stats = run_cuda(c)
+    np.testing.assert_array_equal(s, c["out_states"])
+    np.testing.assert_array_equal(bits(e), bits(c["out_energies"]))
+    assert stats["near_ties"] == 0
+
+
+@pytest.mark.parametrize("mode", ["persistent", "plain"])
+def test_golden_vectors_batched(mode):
+    probs, want = [], []
+    for name in GOLDEN:
+        c = load_golden(name)
+        if bool(c["shared"]):
+            continue
+        probs.append(workloads.Instance(
+            c["h"], c["u"], c["v"], c["J"], np.array(c["states0"], np.int8, copy=True),
+            c["betas"], int(c["spb"]), c["seeds"], bool(c["order"]), CRIT[int(c["proposal"])]))
+        want.append((c["out_states"], c["out_energies"]))
+    stats = {}
+    energies = sample_batch(probs, mode=mode, stats=stats)
+    for p, e, (ws, we) in zip(probs, energies, want):
+        np.testing.assert_array_equal(p.states, ws)
+        np.testing.assert_array_equal(bits(e), bits(we))
+    assert stats["near_ties"] == 0
+    assert stats["attempts"] == sum(p.attempts for p in probs)
+
+
+def _random_problem(rng, n, p=None, degree=None, integer=False):
+    if degree is not None:
+        perm = np.concatenate([rng.permutation(n) for _ in range(degree)])
+        a, b = perm[: len(perm) // 2 * 2].reshape(-1, 2).T
+        ok = a != b
+        u, v = np.minimum(a[ok], b[ok]), np.maximum(a[ok], b[ok])
+    else:
+        iu, ju = np.triu_indices(n, 1)
+        keep = rng.random(iu.shape[0]) < p
+        u, v = iu[keep], ju[keep]
+    J = rng.normal(0, 1, u.shape[0])
+    h = rng.normal(0, 0.1, n)
+    if integer:
+        J = np.sign(J)
+        h = np.zeros(n)
+    return h, u.astype(np.int32), v.astype(np.int32), J
+
+
+@pytest.mark.parametrize("n,kind", [(1, "dense"), (2, "dense"), (31, "dense"), (32, "dense"),
+                                    (33, "dense"), (100, "dense"), (257, "sparse"),
+                                    (1000, "sparse"), (4096, "sparse"), (7000, "sparse")])
+@pytest.mark.parametrize("gibbs", [False, True])
+def test_random_problems_vs_oracle(n, kind, gibbs):
+    rng = np.random.default_rng(n * 2 + gibbs)
+    if kind == "dense":
+        h, u, v, J = _random_problem(rng, n, p=0.5)
+    else:
+        h, u, v, J = _random_problem(rng, n, degree=int(rng.integers(3, 12)))
+    R = 6
+    st = (2 * rng.integers(0, 2, (R, n)) - 1).astype(np.int8)
+    betas = np.geomspace(0.1, 5.0, 60 if n > 1000 else 200)
+    seeds = rng.integers(0, 2**63, R).astype(np.uint64)
+    want_s, want_e = oracle.run(h, u, v, J, st, 1, betas, seeds, False, gibbs)
+    got = st.copy()
+    stats = {}
+    s, e = simulated_annealing(R, h, u, v, J, 1, betas, 0, got, False, CRIT[0 if gibbs else 1],
+                               seeds=seeds, stats=stats)
+    np.testing.assert_array_equal(s, want_s)
+    np.testing.assert_array_equal(bits(e), bits(want_e))
+    assert stats["near_ties"] == 0
+    assert stats["attempts"] == R * len(betas) * n
+
+
+@pytest.mark.parametrize("gibbs", [False, True])
+def test_random_order_vs_oracle(gibbs):
+    rng = np.random.default_rng(55 + gibbs)
+    n = 300
+    h, u, v, J = _random_problem(rng, n, degree=5)
+    st = (2 * rng.integers(0, 2, (8, n)) - 1).astype(np.int8)
+    betas = np.geomspace(0.1, 4.0, 50)
+    seeds = np.arange(10, 18, dtype=np.uint64)
+    want_s, want_e = oracle.run(h, u, v, J, st, 2, betas, seeds, True, gibbs)
+    s, e = simulated_annealing(8, h, u, v, J, 2, betas, 0, st.copy(), True, CRIT[0 if gibbs else 1],
+                               seeds=seeds)
+    np.testing.assert_array_equal(s, want_s)
+    np.testing.assert_array_equal(bits(e), bits(want_e))
+
+
+def test_shared_stream_matches_reference_multiread():
+    rng = np.random.default_rng(9)
+    n = 80
+    h, u, v, J = _random_problem(rng, n, degree=4)
+    st = (2 * rng.integers(0, 2, (12, n)) - 1).astype(np.int8)
+    betas = np.geomspace(0.1, 4.0, 80)
+    want_s, want_e = oracle.run(h, u, v, J, st, 1, betas, [424242], False, False)
+    s, e = simulated_annealing(12, h, u, v, J, 1, betas, 424242, st.copy(), rng_stream="shared")
+    np.testing.assert_array_equal(s, want_s)
+    np.testing.assert_array_equal(bits(e), bits(want_e))
+    # with an interrupt the stream still continues across launches
+    count = [0]
+
+    def stop():
+        count[0] += 1
+        return count[0] >= 7
+
+    s2, e2 = simulated_annealing(12, h, u, v, J, 1, betas, 424242, st.copy(),
+                                 interrupt_function=stop, rng_stream="shared")
+    assert s2.shape == (7, n)
+    np.testing.assert_array_equal(s2, want_s[:7])
+
+
+# ---- tests/test_simulated_annealing.py restated against the CUDA path -------
+
+def fm_problem(num_variables=10, num_samples=100, num_sweeps=1000):
+    # tests/test_simulated_annealing.py:96-122
+    h = [-1] * num_variables
+    cs, ce, cw = zip(*((u, v, -1) for u in range(num_variables) for v in range(u, num_variables)))
+    beta_schedule = np.linspace(0.01, 3, num=num_sweeps)
+    initial_states = (2 * np.random.RandomState(1234).randint(2, size=(num_samples, num_variables))
+                      .astype(np.int8) - 1)
+    return (num_samples, h, cs, ce, cw, 1, beta_schedule, 1, initial_states)
+
+
+@pytest.mark.parametrize("stream", ["per_read", "shared"])
+def test_submit_problem(stream):
+    samples, energies = simulated_annealing(*fm_problem(), rng_stream=stream)
+    assert type(samples) is np.ndarray and samples.shape == (100, 10)
+    assert set(np.unique(samples)).issubset({-1, 1})
+    assert type(energies) is np.ndarray and energies.shape == (100,)
+
+
+@pytest.mark.parametrize("stream", ["per_read", "shared"])
+def test_good_results(stream):
+    samples, energies = simulated_annealing(*fm_problem(num_variables=5), rng_stream=stream)
+    ground_energy = -(5 + 3) * 5 / 2  # pins the self-loop semantics
+    assert [1] * 5 in samples.tolist()
+    assert abs(np.mean(energies) - ground_energy) <= 2
+
+
+def test_seed_determinism():
+    n, sweeps, R = 100, 10, 1000
+    cs, ce, cw = zip(*((u, v, 1) for u in range(n) for v in range(u, n)))
+    betas = np.linspace(0.3, 0.4, num=sweeps)
+    init = 2 * np.random.RandomState(1234).randint(1, size=(R, n)).astype(np.int8) - 1
+    prev = []
+    for seed in (1, 40, 235, 152436, 3462354, 92352355):
+        a, _ = simulated_annealing(R, [0] * n, cs, ce, cw, 1, betas, seed, np.copy(init))
+        b, _ = simulated_annealing(R, [0] * n, cs, ce, cw, 1, betas, seed, np.copy(init))
+        assert np.array_equal(a, b)
+        for p in prev:
+            assert not np.array_equal(a, p)
+        prev.append(a)
+
+
+@pytest.mark.parametrize("stream", ["per_read", "shared"])
+def test_interrupts(stream):
+    prob = fm_problem(num_variables=5)
+    s, e = simulated_annealing(*prob, interrupt_function=lambda: True, rng_stream=stream)
+    assert s.shape == (1, 5) and e.shape == (1,)
+    count = [1]
+
+    def stop():
+        if count[0] >= 5:
+            return True
+        count[0] += 1
+        return False
+
+    init = prob[-1].copy()
+    s, e = simulated_annealing(*prob, interrupt_function=stop, rng_stream=stream)
+    assert s.shape == (5, 5) and e.shape == (5,)
+    # rows past the stop keep their initial states, as in the reference
+    np.testing.assert_array_equal(prob[-1][5:], init[5:])
+
+    def boom():
+        raise RuntimeError("x")
+
+    s, e = simulated_annealing(*prob, interrupt_function=boom, rng_stream=stream)
+    assert s.shape == (1, 5)
+
+
+def test_zero_sweeps_returns_initial_states():
+    n, R = 100, 1000
+    cs, ce, cw = zip(*((u, v, 1) for u in range(n) for v in range(u, n)))
+    init = 2 * np.random.RandomState(1234).randint(1, size=(R, n)).astype(np.int8) - 1
+    s, _ = simulated_annealing(R, [0] * n, cs, ce, cw, 1, np.linspace(0.3, 0.4, num=0),
+                               1234567890, np.copy(init))
+    assert np.array_equal(init, s)
+
+
+def test_concurrent_calls_from_threads():
+    prob = fm_problem(num_variables=60, num_samples=64, num_sweeps=2000)
+    ref, _ = simulated_annealing(*[np.copy(x) if isinstance(x, np.ndarray) else x for x in prob])
+    out = [None, None]
+
+    def work(i):
+        p = [np.copy(x) if isinstance(x, np.ndarray) else x for x in prob]
+        out[i] = simulated_annealing(*p)[0]
+
+    ts = [threading.Thread(target=work, args=(i,)) for i in range(2)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    assert np.array_equal(out[0], ref) and np.array_equal(out[1], ref)
+
+
+# ---- sampler-level behaviour (tests/test_simulated_annealing_sampler.py:659-846)
+
+def test_metropolis_null_model_oscillates():
+    n = 100
+    init = (1 - 2 * np.random.randint(2, size=n)).astype(np.int8)
+    for sweeps in range(3):
+        st = init[None, :].copy()
+        s, _ = simulated_annealing(1, [0.0] * n, [], [], [], 1,
+                                   np.geomspace(0.1, 1.0, sweeps) if sweeps > 1 else
+                                   np.array([1.0] * sweeps), 7, st)
+        assert np.all(s[0] == (-1) ** sweeps * init)
+
+
+def test_greedy_limit_beta_inf():
+    n = 10000
+    hv = np.random.default_rng(3).normal(size=n)
+    ground = (-np.sign(hv)).astype(np.int8)
+    for crit in ("Metropolis", "Gibbs"):
+        for init in (ground, -ground):
+            s, _ = simulated_annealing(1, hv, [], [], [], 1, [np.inf], 2023,
+                                       init[None, :].copy(), False, crit)
+            assert np.all(s[0] == ground)
+
+
+# ---- full-size lattice (3D periodic L=32), sampled reads vs the oracle -----
+
+def test_cubic_lattice_full_size():
+    inst = workloads.cubic_lattice(L=32, reads=16, sweeps=4096)
+    st = inst.states.copy()
+    stats = {}
+    s, e = simulated_annealing(16, inst.h, inst.u, inst.v, inst.J, 1, inst.betas, 0, st,
+                               seeds=inst.seeds, stats=stats)
+    assert stats["near_ties"] == 0 and stats["attempts"] == 16 * 4096 * 32768
+    for r in range(16):  # energy consistency for every read
+        assert e[r] == oracle.energy(inst.h, inst.u, inst.v, inst.J, s[r])
+    for r in (0, 11):   # two reads replayed on the CPU oracle
+        ws, we = oracle.run(inst.h, inst.u, inst.v, inst.J, inst.states[r:r + 1], 1,
+                            inst.betas, inst.seeds[r:r + 1])
+        np.testing.assert_array_equal(s[r], ws[0])
+        assert bits(e[r:r + 1])[0] == bits(we)[0]
+
+
+def test_uneven_batch_small_persistent_vs_plain_vs_oracle():
+    probs = workloads.uneven_batch(num_problems=12, n_range=(64, 700), reads_range=(3, 40),
+                                   sweeps_range=(20, 120), seed=17)
+    import copy
+    a = copy.deepcopy(probs)
+    b = copy.deepcopy(probs)
+    ea = sample_batch(a, mode="persistent")
+    eb = sample_batch(b, mode="plain")
+    for pa, pb, xa, xb in zip(a, b, ea, eb):
+        np.testing.assert_array_equal(pa.states, pb.states)
+        np.testing.assert_array_equal(bits(xa), bits(xb))
+    for p, pa, xa in list(zip(probs, a, ea))[:4]:
+        ws, we = oracle.run(p.h, p.u, p.v, p.J, p.states, 1, p.betas, p.seeds)
+        np.testing.assert_array_equal(pa.states, ws)
+        np.testing.assert_array_equal(bits(xa), bits(we))
+
+
+def test_plan_device_buffers_repeatable():
+    import torch
+    probs = workloads.uneven_batch(num_problems=5, n_range=(64, 300), reads_range=(4, 16),
+                                   sweeps_range=(10, 40), seed=23)
+    with Plan(probs) as plan:
+        host = np.concatenate([p.states.ravel() for p in probs])
+        sin = torch.from_numpy(host).cuda()
+        out1 = torch.empty_like(sin)
+        out2 = torch.empty_like(sin)
+        en1 = torch.empty(plan.total_reads, dtype=torch.float64, device="cuda")
+        en2 = torch.empty_like(en1)
+        plan.run(sin, out1, en1)
+        st = plan.run(sin, out2, en2, mode="plain")
+        assert torch.equal(out1, out2) and torch.equal(en1, en2)
+        assert torch.equal(sin.cpu(), torch.from_numpy(host))  # input untouched
+        assert st["attempts"] == plan.attempts
+        p0 = probs[0]
+        ws, we = oracle.run(p0.h, p0.u, p0.v, p0.J, p0.states, 1, p0.betas, p0.seeds)
+        got = out1[: p0.num_reads * p0.n].cpu().numpy().reshape(p0.num_reads, p0.n)
+        np.testing.assert_array_equal(got, ws)

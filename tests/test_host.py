@@ -1,0 +1,224 @@
+"""Host-side logic that needs no GPU: argument handling of the drop-in
+binding, seed mapping, workload generators, and a CPU model of the kernel's
+speculative-window and RNG-ring algorithm checked against the oracle."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from b200sa import per_read_seeds, simulated_annealing
+from b200sa import workloads
+
+
+def test_empty_short_circuit():
+    # simulated_annealing.pyx:134-136
+    s, e = simulated_annealing(0, [1.0, 2.0], [], [], [], 1, [1.0], 1,
+                               np.ones((0, 2), np.int8))
+    assert s.shape == (0, 2) and e.shape == (0,)
+    s, e = simulated_annealing(3, [], [], [], [], 1, [1.0], 1, np.ones((3, 0), np.int8))
+    assert s.shape == (3, 0) and s.dtype == np.int8
+    assert np.array_equal(e, np.zeros(3))
+
+
+def test_argument_errors_match_reference():
+    st = np.ones((2, 3), np.int8)
+    h = [0.0, 0.0, 0.0]
+    with pytest.raises(ValueError, match="Unknown proposal_acceptance_criteria"):
+        simulated_annealing(2, h, [0], [1], [1.0], 1, [1.0], 1, st,
+                            proposal_acceptance_criteria="heatbath")
+    with pytest.raises(OverflowError):
+        simulated_annealing(2, h, [0], [1], [1.0], 1, [1.0], -1, st)
+    with pytest.raises(ValueError, match="mismatched"):
+        simulated_annealing(2, h, [0, 1], [1], [1.0], 1, [1.0], 1, st)
+    with pytest.raises(ValueError, match="dtype"):
+        simulated_annealing(2, h, [0], [1], [1.0], 1, [1.0], 1, st.astype(np.int16))
+    with pytest.raises(ValueError, match="C-contiguous"):
+        simulated_annealing(2, h, [0], [1], [1.0], 1, [1.0], 1,
+                            np.ones((3, 2), np.int8).T)
+    with pytest.raises(ValueError, match="shape"):
+        simulated_annealing(3, h, [0], [1], [1.0], 1, [1.0], 1, st)
+
+
+def test_per_read_seeds_wrap():
+    s = per_read_seeds(2**64 - 2, 4)
+    assert list(map(int, s)) == [2**64 - 2, 2**64 - 1, 0, 1]
+    assert list(map(int, per_read_seeds(5, 3))) == [5, 6, 7]
+
+
+def test_workload_shapes():
+    d = workloads.dense_ising(n=40, reads=3, sweeps=7)
+    assert d.states.shape == (3, 40) and len(d.betas) == 7
+    assert np.all(d.u < d.v) and d.attempts == 3 * 7 * 40
+    lat = workloads.cubic_lattice(L=4, reads=2, sweeps=5)
+    deg = np.bincount(np.concatenate([lat.u, lat.v]), minlength=64)
+    assert lat.n == 64 and np.all(deg == 6) and set(np.unique(lat.J)) <= {-1.0, 1.0}
+    b = workloads.uneven_batch(num_problems=3, n_range=(64, 128), reads_range=(4, 8),
+                               sweeps_range=(16, 32))
+    assert len(b) == 3
+    for p in b:
+        deg = np.bincount(np.concatenate([p.u, p.v]), minlength=p.n)
+        assert len(set(deg.tolist())) == 1 and 3 <= deg[0] <= 16
+        assert p.seeds.shape == (p.num_reads,)
+    k = workloads.complete_graph(reads=5, sweeps=3)
+    assert k.n == 16 and k.J.shape == (120,) and k.proposal == "Gibbs"
+
+
+# ---- CPU model of the kernel algorithm -------------------------------------
+M64 = (1 << 64) - 1
+RING, HALF, PER = 512, 256, 8
+
+
+def _adv(s0, s1):
+    a, b = s0, s1
+    s0 = b
+    a = (a ^ (a << 23)) & M64
+    return s0, a ^ b ^ (a >> 17) ^ (b >> 26)
+
+
+def _jump_columns(steps):
+    cols = []
+    for bit in range(128):
+        s0 = (1 << bit) if bit < 64 else 0
+        s1 = 0 if bit < 64 else 1 << (bit - 64)
+        for _ in range(steps):
+            s0, s1 = _adv(s0, s1)
+        cols.append((s0, s1))
+    return cols
+
+
+class _Ring:
+    """The kernel's ring: 32 lanes each fill PER consecutive outputs per half,
+    then jump their segment state HALF steps with the GF(2) matrix."""
+    cols = None
+
+    def __init__(self, seed):
+        if _Ring.cols is None:
+            _Ring.cols = _jump_columns(HALF)
+        self.ring = [0] * RING
+        s0, s1 = (seed or M64), 0
+        self.T = []
+        for lane in range(32):
+            a, b = s0, s1
+            for _ in range(lane * PER):
+                a, b = _adv(a, b)
+            self._fill(0, a, b, lane)
+            a, b = self._jump(a, b)
+            self._fill(HALF, a, b, lane)
+            self.T.append(self._jump(a, b))
+        self.q = self.base = 0
+
+    def _jump(self, s0, s1):
+        a0 = a1 = 0
+        for bit in range(128):
+            if ((s0 if bit < 64 else s1) >> (bit % 64)) & 1:
+                a0 ^= self.cols[bit][0]
+                a1 ^= self.cols[bit][1]
+        return a0, a1
+
+    def _fill(self, pos, a, b, lane):
+        for t in range(PER):
+            prev = b
+            a, b = _adv(a, b)
+            self.ring[(pos + lane * PER + t) & (RING - 1)] = (b + prev) & M64
+
+    def refill(self):
+        if self.q - self.base >= HALF:
+            for lane in range(32):
+                a, b = self.T[lane]
+                self._fill(self.base + RING, a, b, lane)
+                self.T[lane] = self._jump(a, b)
+            self.base += HALF
+
+    def get(self, pos):
+        assert self.base <= pos < self.base + RING
+        return self.ring[pos & (RING - 1)]
+
+
+def test_ring_reproduces_stream():
+    want = oracle.rng_stream(987654321, 3000)
+    r = _Ring(987654321)
+    got = []
+    while r.q < 3000:
+        r.refill()
+        take = min(29, 3000 - r.q)
+        got += [r.get(r.q + i) for i in range(take)]
+        r.q += take
+    assert got == list(map(int, want))
+
+
+def _model_anneal(h, u, v, J, s, betas, spb, seed, gibbs):
+    """Speculative 32-wide windows exactly as the sequential-order kernel."""
+    n = len(h)
+    rows = [[] for _ in range(n)]
+    for a, b, w in zip(u, v, J):
+        rows[a].append((int(b), float(w)))
+        rows[b].append((int(a), float(w)))
+    dist = []
+    for i in range(n):
+        ds = [t - i for t, _ in rows[i] if t > i]
+        dist.append(min([32] + ds))
+    s = [int(x) for x in s]
+    de = []
+    for i in range(n):
+        f = float(h[i])
+        for t, w in rows[i]:
+            f += s[t] * w
+        de.append((-2 * s[i]) * f)
+    R = _Ring(seed)
+    for beta in betas:
+        thr = 44.36142 / beta
+        for _ in range(spb):
+            p = 0
+            while p < n:
+                R.refill()
+                L = min(32, n - p)
+                need, acc = [False] * L, [False] * L
+                for k in range(L):
+                    d = de[p + k]
+                    consider = not (d >= thr)
+                    need[k] = consider if gibbs else (consider and not d <= 0.0)
+                    acc[k] = (not gibbs) and consider
+                c = 0
+                for k in range(L):
+                    if need[k]:
+                        r = float(R.get(R.q + c))
+                        c += 1
+                        d = de[p + k]
+                        if gibbs:
+                            e = math.exp(d * beta) if d * beta < 709 else math.inf
+                            acc[k] = 2.0 ** 64 > r * (1 + e)
+                        else:
+                            acc[k] = math.exp(-d * beta) * 2.0 ** 64 > r
+                commit = min([L] + [k + dist[p + k] for k in range(L) if acc[k]])
+                R.q += sum(need[:commit])
+                for k in range(commit):
+                    if acc[k]:
+                        var = p + k
+                        m = float(np.int8(4 * s[var]))
+                        for t, w in rows[var]:
+                            de[t] += m * w * s[t]
+                        s[var] = -s[var]
+                        de[var] = -de[var]
+                p += commit
+    return np.array(s, np.int8)
+
+
+@pytest.mark.parametrize("gibbs", [False, True])
+def test_speculative_window_model_matches_oracle(gibbs):
+    rng = np.random.default_rng(7 + gibbs)
+    for n, p in ((45, 0.08), (70, 0.5)):
+        iu, ju = np.triu_indices(n, 1)
+        keep = rng.random(iu.shape[0]) < p
+        u = np.concatenate([iu[keep], [3, 9]]).astype(np.int32)   # a self-loop and a duplicate
+        v = np.concatenate([ju[keep], [3, ju[keep][0]]]).astype(np.int32)
+        u[-1] = iu[keep][0]
+        J = rng.uniform(-1, 1, u.shape[0])
+        h = rng.uniform(-1, 1, n)
+        betas = np.geomspace(0.1, 4.0, 25)
+        st = (2 * rng.integers(0, 2, (2, n)) - 1).astype(np.int8)
+        seeds = np.array([3, 0], np.uint64)
+        want, _ = oracle.run(h, u, v, J, st, 1, betas, seeds, False, gibbs)
+        for r in range(2):
+            got = _model_anneal(h, u, v, J, st[r], betas, 1, int(seeds[r]), gibbs)
+            np.testing.assert_array_equal(got, want[r])
