@@ -51,12 +51,19 @@ def parse_args():
     ap.add_argument("--cpu-budget", type=float, default=15.0,
                     help="seconds of CPU baseline sampling on rank 0")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--sweep-scale", type=float, default=1.0,
+                    help="scale every schedule's length (profiling captures only; "
+                         "1.0 is the benchmark workload)")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
 
 
 def workload(args, rank=0):
     probs = workloads.uneven_batch(num_problems=args.problems)
+    if args.sweep_scale != 1.0:
+        for p in probs:
+            k = max(1, int(round(len(p.betas) * args.sweep_scale)))
+            p.betas = np.geomspace(0.1, 5.0, k)
     if rank:  # weak scaling: same shapes, rank-specific read seeds
         for p in probs:
             p.seeds = p.seeds + np.uint64(rank * (1 << 32))
@@ -144,14 +151,30 @@ def cpu_sample(probs, budget_s, threads=None, max_reads=None):
 
 # ------------------------------------------------------------- GPU helpers --
 
+def gpu_selector(device):
+    """nvidia-smi -i argument for a torch device: its UUID when available
+    (the visible device need not be physical GPU `device`)."""
+    try:
+        import torch
+        uuid = str(torch.cuda.get_device_properties(device).uuid)
+        if uuid:
+            return uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+    except Exception:
+        pass
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        return vis.split(",")[device].strip()
+    return str(device)
+
+
 class Clocks:
     """Samples SM clock and throttle reasons with nvidia-smi while running."""
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
-        self.index = index
+    def __init__(self, device):
+        self.index = gpu_selector(device)
         self.proc = None
         self.lines = []
 
@@ -310,7 +333,7 @@ def run_ours(args):
     sin = torch.from_numpy(host_states).cuda()
     sout = torch.empty_like(sin)
     en = torch.empty(plan.total_reads, dtype=torch.float64, device="cuda")
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()
 
     def timed(mode, warmup, steps):
         for _ in range(warmup):
@@ -337,6 +360,8 @@ def run_ours(args):
     # Counters of one run (deterministic for these inputs).
     stats = plan.run(sin, sout, en, mode="persistent", stream=stream, sync=True)
     flips = stats["flips"]
+    if stats["attempts"] != attempts:
+        raise RuntimeError(f"attempt count mismatch: {stats['attempts']} != {attempts}")
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -354,7 +379,8 @@ def run_ours(args):
     line["clocks"] = clk.summary()
     line["gpu_launches"] = args.steps
     line["counters"] = {"flips": flips, "near_ties": stats["near_ties"],
-                        "attempts_per_pass": attempts / max(stats["passes"], 1)}
+                        "attempts_per_pass": attempts / max(stats["passes"], 1),
+                        "check_run_kernel_ms": stats["kernel_ms"]}
 
     if not args.no_plain:
         plain_ms = max_over_ranks(timed("plain", 1, args.plain_steps)) / args.plain_steps
@@ -365,7 +391,7 @@ def run_ours(args):
     # End to end through the C ABI with host buffers (pack + H2D + anneal + D2H).
     bi, bo = h2d_d2h_bytes(probs)
     e2e_times = []
-    for _ in range(args.e2e_steps + 1):
+    for _ in range(args.e2e_steps + 1 if args.e2e_steps > 0 else 0):
         work = [copy.copy(p) for p in probs]
         for w in work:
             w.states = w.states.copy()
@@ -375,9 +401,10 @@ def run_ours(args):
         sample_batch(work, mode="persistent", device=local)
         dt = time.perf_counter() - t0
         e2e_times.append(max_over_ranks(dt))
-    e2e = statistics.median(e2e_times[1:])
-    line["e2e"] = {"value": world * attempts / e2e, "unit": UNIT, "h2d_bytes_per_step": bi,
-                   "d2h_bytes_per_step": bo, "seconds_per_step": e2e}
+    if e2e_times:
+        e2e = statistics.median(e2e_times[1:])
+        line["e2e"] = {"value": world * attempts / e2e, "unit": UNIT, "h2d_bytes_per_step": bi,
+                       "d2h_bytes_per_step": bo, "seconds_per_step": e2e}
 
     if rank == 0 and not args.no_cpu:
         cb = cpu_sample(probs, args.cpu_budget)

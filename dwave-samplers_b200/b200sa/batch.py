@@ -17,6 +17,7 @@ from . import _lib
 from .workloads import Instance
 
 MODES = {"persistent": _lib.MODE_PERSISTENT, "plain": _lib.MODE_PLAIN}
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 
 
 def _proposal_code(p: str) -> int:
@@ -130,6 +131,8 @@ class Plan:
         s = None
         if stream is not None:
             s = stream if isinstance(stream, int) else stream.cuda_stream
+            if s == 0:  # the legacy default stream: pass cudaStreamLegacy, not NULL
+                s = CUDA_STREAM_LEGACY
         rc = self._lib.b200sa_plan_run(self.handle, MODES[mode], ptr(states_in),
                                        ptr(states_out), ptr(energies), ptr(seeds), s,
                                        1 if sync else 0, ctypes.byref(st), err, len(err))

@@ -43,6 +43,7 @@ int validate_problem(const b200sa_problem &p, std::string &msg) {
         return B200SA_EINVAL;
     }
     // cpu_sa.cpp:302-304 (the reference throws; here it is an error code).
+    std::vector<uint32_t> deg((size_t)std::max(p.num_vars, 0), 0);
     for (int64_t c = 0; c < p.num_couplers; ++c) {
         const int32_t a = p.coupler_starts[c], b = p.coupler_ends[c];
         if (a < 0 || b < 0 || a >= p.num_vars || b >= p.num_vars) {
@@ -51,6 +52,10 @@ int validate_problem(const b200sa_problem &p, std::string &msg) {
                           "(coupler %lld: %d, %d; num_vars %d)",
                           (long long)c, a, b, p.num_vars);
             msg = buf;
+            return B200SA_EINVAL;
+        }
+        if (++deg[a] > kMaxDegree || ++deg[b] > kMaxDegree) {
+            msg = "a variable has more than 2^24-1 adjacency entries";
             return B200SA_EINVAL;
         }
     }
@@ -63,7 +68,7 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
     out.row.assign((size_t)n + 1, 0);
     out.col.resize((size_t)(2 * m));
     out.w.resize((size_t)(2 * m));
-    out.vinfo.assign((size_t)n, 0);
+    out.vinfo.assign((size_t)n * 2, 0);
     for (int64_t c = 0; c < m; ++c) {
         out.row[(size_t)p.coupler_starts[c] + 1]++;
         out.row[(size_t)p.coupler_ends[c] + 1]++;
@@ -82,26 +87,47 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
         out.col[k] = a;
         out.w[k] = J;
     }
-    // Speculation info: nearest later neighbour and repeated targets.
+    // Speculation info: nearest later neighbour; repeated targets; pairs of
+    // variables less than 32 apart with a common neighbour.
+    out.share.assign((size_t)n, 0u);
+    {
+        std::vector<int32_t> nb;
+        for (int32_t u = 0; u < n; ++u) {
+            nb.assign(out.col.begin() + out.row[u], out.col.begin() + out.row[u + 1]);
+            std::sort(nb.begin(), nb.end());
+            nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
+            for (size_t i = 0; i < nb.size(); ++i)
+                for (size_t j = i + 1; j < nb.size() && nb[j] - nb[i] < 32; ++j)
+                    out.share[nb[i]] |= 1u << (nb[j] - nb[i]);
+        }
+    }
     std::vector<int32_t> mark((size_t)n, -1);
     int32_t maxdeg = 0;
     bool any_dup = false;
     for (int32_t v = 0; v < n; ++v) {
-        int32_t dist = 32;
-        bool dup = false;
+        uint32_t dist = 32;
         const int32_t e0 = out.row[v], e1 = out.row[v + 1];
         maxdeg = std::max(maxdeg, e1 - e0);
         for (int32_t e = e0; e < e1; ++e) {
             const int32_t u = out.col[e];
-            if (u > v) dist = std::min(dist, u - v);
-            if (mark[u] == v) dup = true;
+            if (u > v) dist = std::min<uint32_t>(dist, (uint32_t)(u - v));
+            if (mark[u] == v) {
+                any_dup = true;
+                out.share[v] |= 1u;
+            }
             mark[u] = v;
         }
-        out.vinfo[v] = (uint8_t)((dist & kDistMask) | (dup ? kDupFlag : 0));
-        any_dup |= dup;
+        out.vinfo[2 * (size_t)v] = (uint32_t)e0;
+        out.vinfo[2 * (size_t)v + 1] = (uint32_t)(e1 - e0) | (dist << kDistShift);
     }
     out.max_degree = maxdeg;
     out.any_dup = any_dup;
+    out.regular_degree = 0;
+    if (n > 0 && maxdeg > 0 && maxdeg <= 32) {
+        bool reg = true;
+        for (int32_t v = 0; v < n && reg; ++v) reg = (out.row[v + 1] - out.row[v]) == maxdeg;
+        if (reg) out.regular_degree = maxdeg;
+    }
 }
 
 // One xorshift128+ state transition (cpu_sa.cpp:27-34 without the output).
@@ -122,6 +148,19 @@ void rng_jump_columns(int64_t steps, uint32_t out[128][4]) {
         out[bit][1] = (uint32_t)(s0 >> 32);
         out[bit][2] = (uint32_t)s1;
         out[bit][3] = (uint32_t)(s1 >> 32);
+    }
+}
+
+void rng_jump_nibbles(const uint32_t cols[128][4], uint32_t out[][4]) {
+    for (int k = 0; k < kJumpNibbles; ++k) {
+        for (int v = 0; v < 16; ++v) {
+            uint32_t acc[4] = {0, 0, 0, 0};
+            for (int b = 0; b < 4; ++b) {
+                if (!((v >> b) & 1)) continue;
+                for (int w = 0; w < 4; ++w) acc[w] ^= cols[4 * k + b][w];
+            }
+            for (int w = 0; w < 4; ++w) out[k * 16 + v][w] = acc[w];
+        }
     }
 }
 

@@ -9,16 +9,18 @@
 namespace b200sa {
 
 struct PackedAdjacency {
-    std::vector<int32_t> row;    // n+1
-    std::vector<int32_t> col;    // 2m
-    std::vector<double> w;       // 2m
-    std::vector<uint8_t> vinfo;  // n
+    std::vector<int32_t> row;     // n+1
+    std::vector<int32_t> col;     // 2m
+    std::vector<double> w;        // 2m
+    std::vector<uint32_t> vinfo;  // 2n: per variable {list start, degree | dist << 24}
+    std::vector<uint32_t> share;  // n: conflict mask (see ProblemDev::share)
     int32_t max_degree = 0;
-    bool any_dup = false;
+    int32_t regular_degree = 0;   // common list length when all lists are equally long
+    bool any_dup = false;         // some list names a target twice (self-loop / repeat)
 };
 
-// Validates one problem's arguments (lengths, indices, enums).  Returns
-// B200SA_OK or B200SA_EINVAL with a message.
+// Validates one problem's arguments (lengths, indices, enums, degree limit).
+// Returns B200SA_OK or B200SA_EINVAL with a message.
 int validate_problem(const b200sa_problem &p, std::string &msg);
 
 // Order-preserving adjacency, same order as cpu_sa.cpp:298-316.
@@ -29,5 +31,9 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out);
 // set (bits 0-63 = word 0, 64-127 = word 1).  Four uint32 words per column:
 // word0 lo, word0 hi, word1 lo, word1 hi.
 void rng_jump_columns(int64_t steps, uint32_t out[128][4]);
+
+// Nibble tables of that matrix: out[k*16 + v] (four words each) is the XOR of
+// the columns selected by the bits of v at nibble position k.
+void rng_jump_nibbles(const uint32_t cols[128][4], uint32_t out[][4]);
 
 }  // namespace b200sa

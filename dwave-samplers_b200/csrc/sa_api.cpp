@@ -9,9 +9,11 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
-#include <numeric>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "b200sa.h"
@@ -24,9 +26,7 @@ using namespace b200sa;
 namespace {
 
 int set_err(char *err, size_t errlen, int code, const std::string &msg) {
-    if (err && errlen > 0) {
-        std::snprintf(err, errlen, "%s", msg.c_str());
-    }
+    if (err && errlen > 0) std::snprintf(err, errlen, "%s", msg.c_str());
     return code;
 }
 
@@ -41,7 +41,12 @@ int set_err(char *err, size_t errlen, int code, const std::string &msg) {
 // Restores the caller's current device on scope exit.
 struct DeviceGuard {
     int prev = -1;
-    DeviceGuard() { cudaGetDevice(&prev); }
+    DeviceGuard() {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            prev = -1;
+            cudaGetLastError();
+        }
+    }
     ~DeviceGuard() {
         if (prev >= 0) cudaSetDevice(prev);
     }
@@ -88,15 +93,36 @@ struct DevArray {
 
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
-const uint32_t (*jump_columns())[4] {
-    static uint32_t cols[128][4];
-    static bool ready = false;
-    if (!ready) {  // idempotent; concurrent first calls write identical values
+const uint32_t (*jump_table())[4] {
+    static uint32_t table[kJumpTable][4];
+    static std::once_flag once;
+    std::call_once(once, [] {
+        uint32_t cols[128][4];
         rng_jump_columns(kHalf, cols);
-        ready = true;
-    }
-    return cols;
+        rng_jump_nibbles(cols, table);
+    });
+    return table;
 }
+
+// Buckets of the persistent mode: a size class crossed with the kernel kind
+// (acceptance rule x update order).  Each bucket's warps get a shared region
+// sized for the bucket's largest n, so small problems pack more resident
+// warps per SM; the last size class keeps its state in global memory.
+constexpr int kSizeClasses = 8;
+constexpr int kGlobalClass = kSizeClasses - 1;
+constexpr int kKinds = 4;
+constexpr int kBuckets = kSizeClasses * kKinds;
+constexpr int kStreams = 8;
+const int kClassBound[kSizeClasses - 2] = {128, 256, 512, 1024, 2048, 4096};
+
+int size_class(int n, int onchip_max) {
+    if (n > onchip_max) return kGlobalClass;
+    for (int b = 0; b < kSizeClasses - 2; ++b)
+        if (n <= kClassBound[b]) return b;
+    return kSizeClasses - 2;
+}
+
+int kind_of(const ProblemDev &d) { return (d.proposal == 0 ? 1 : 0) | (d.varorder ? 2 : 0); }
 
 }  // namespace
 
@@ -104,8 +130,11 @@ struct b200sa_plan_s {
     int device = 0;
     cudaDeviceProp prop{};
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t bstream[kStreams] = {};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
+    cudaEvent_t join[kStreams] = {};
     int num_problems = 0;
+    int onchip_max = 0;
     std::vector<ProblemDev> hprobs;
     std::vector<int32_t> n, reads, sweeps;  // per problem
     std::vector<int64_t> state_off, read_off;
@@ -116,16 +145,25 @@ struct b200sa_plan_s {
     DevArray<uint64_t> dseeds;
     DevArray<ReadStats> dstats;
     DevArray<int64_t> items_lpt, items_plain;
-    DevArray<unsigned long long> qhead;
+    DevArray<unsigned long long> qhead;  // one per bucket
     DevArray<double> scratch_de;
     DevArray<int8_t> scratch_s;
     DevArray<uint64_t> carry;
     int64_t scratch_stride = 0, scratch_slots = 0;
-    std::vector<int64_t> plain_item_off;  // per problem offset into items_plain
+    std::vector<int64_t> plain_item_off;   // per problem offset into items_plain
+    int64_t bucket_off[kBuckets + 1] = {};  // bucket ranges in items_lpt
+    int32_t bucket_max_n[kBuckets] = {};
+    int64_t bucket_lead_cost[kBuckets] = {};
+    std::map<std::pair<int, int>, int> occ_cache;  // (variant*2^24 + warps, region) -> CTAs/SM
 
     ~b200sa_plan_s() {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (fork) cudaEventDestroy(fork);
+        for (int b = 0; b < kStreams; ++b) {
+            if (join[b]) cudaEventDestroy(join[b]);
+            if (bstream[b]) cudaStreamDestroy(bstream[b]);
+        }
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -137,30 +175,56 @@ struct LaunchShape {
     int warps_per_cta;
     int region;
     int grid;
+    int variant;
 };
 
-// Chooses how many warps share a CTA and which problems keep their state in
-// shared memory.  Every warp anneals one read at a time; a warp's shared
-// region holds the RNG ring plus, when n <= cap_n, the read's delta energies
-// and spins.  Larger problems keep those in a global slot (L2-resident).
-int shape_for(b200sa_plan_s *P, int32_t max_n_here, int64_t items, bool persistent,
+int occupancy(b200sa_plan_s *P, int variant, int w, int region, int *ctas, char *err,
+              size_t errlen) {
+    auto key = std::make_pair((variant << 24) + w, region);
+    auto it = P->occ_cache.find(key);
+    if (it != P->occ_cache.end()) {
+        *ctas = it->second;
+        return B200SA_OK;
+    }
+    B200SA_CUDA(kernel_occupancy(variant, w, region, ctas));
+    P->occ_cache[key] = *ctas;
+    return B200SA_OK;
+}
+
+// Every warp anneals one read at a time; its shared region holds the RNG
+// ring, the conflict scratch and, when n <= cap_n, the read's delta energies
+// and spins (else those live in a global slot, L2-resident).  Warps per CTA
+// are chosen to maximize resident warps per SM.
+int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, bool persistent,
               LaunchShape &out, char *err, size_t errlen) {
-    const int smem_sm = (int)P->prop.sharedMemPerMultiprocessor;
     const int smem_blk = (int)P->prop.sharedMemPerBlockOptin;
-    // Keep at least 4 resident warps per SM when the state lives on chip.
-    int cap = max_n_here;
-    if (region_bytes_for(cap) * 4 > smem_sm) cap = 0;
+    const int cap = max_n_here <= P->onchip_max ? max_n_here : 0;
     const int region = region_bytes_for(cap);
-    int w = std::max(1, std::min(kMaxThreadsPerCta / 32, smem_blk / region));
-    if (!persistent) w = std::min<int64_t>(w, std::max<int64_t>(1, items));
-    int per_sm = 0;
-    B200SA_CUDA(kernel_occupancy(w, region, &per_sm));
-    if (per_sm < 1) return set_err(err, errlen, B200SA_ECUDA, "kernel does not fit on an SM");
+    const int variant = kernel_variant(kind & 1, kind & 2, cap > 0);
+    int best_w = 1, best_warps = 0;
+    for (int w = 1; w <= kMaxThreadsPerCta / 32; ++w) {
+        if ((int64_t)w * region > smem_blk) break;
+        int ctas = 0;
+        int rc = occupancy(P, variant, w, region, &ctas, err, errlen);
+        if (rc) return rc;
+        if (ctas * w > best_warps) {
+            best_warps = ctas * w;
+            best_w = w;
+        }
+    }
+    if (best_warps == 0)
+        return set_err(err, errlen, B200SA_ECUDA, "kernel does not fit on an SM");
+    // Fewer items than resident warp slots: spread them over every SM first.
+    const int sms = P->prop.multiProcessorCount;
+    int w = (int)std::min<int64_t>(best_w, std::max<int64_t>(1, (items + sms - 1) / sms));
     int grid;
     if (persistent) {
-        grid = P->prop.multiProcessorCount * per_sm;
-        const int64_t need = (items + w - 1) / w;
-        grid = (int)std::max<int64_t>(1, std::min<int64_t>(grid, need));
+        int ctas = best_warps / best_w;
+        if (w != best_w) {
+            int rc = occupancy(P, variant, w, region, &ctas, err, errlen);
+            if (rc) return rc;
+        }
+        grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * ctas, (items + w - 1) / w));
     } else {
         grid = (int)std::max<int64_t>(1, (items + w - 1) / w);
     }
@@ -168,6 +232,7 @@ int shape_for(b200sa_plan_s *P, int32_t max_n_here, int64_t items, bool persiste
     out.warps_per_cta = w;
     out.region = region;
     out.grid = grid;
+    out.variant = variant;
     return B200SA_OK;
 }
 
@@ -196,15 +261,15 @@ LaunchArgs base_args(b200sa_plan_s *P, const int8_t *in, int8_t *out, double *en
     return a;
 }
 
-// Runs the items [first, first+count) of problem `pi`'s read-ordered list (plain
-// list) or the whole LPT list (persistent) with one launch.
-int launch_items(b200sa_plan_s *P, LaunchArgs a, const int64_t *items, int64_t count,
-                 int32_t max_n_here, bool persistent, bool shared_stream,
-                 cudaStream_t st, char *err, size_t errlen) {
+// One launch over `count` items.  Persistent launches take items from the
+// work-queue head `qhead` (zeroed by the caller, stream-ordered).
+int launch_items(b200sa_plan_s *P, LaunchArgs a, int kind, const int64_t *items,
+                 int64_t count, int32_t max_n_here, bool persistent, bool shared_stream,
+                 unsigned long long *qhead, cudaStream_t st, char *err, size_t errlen) {
     if (count <= 0) return B200SA_OK;
     LaunchShape s{};
-    int rc = shape_for(P, max_n_here, shared_stream ? 1 : count, persistent && !shared_stream,
-                       s, err, errlen);
+    int rc = shape_for(P, kind, max_n_here, shared_stream ? 1 : count,
+                       persistent && !shared_stream, s, err, errlen);
     if (rc) return rc;
     if (shared_stream) {
         s.grid = 1;
@@ -221,11 +286,8 @@ int launch_items(b200sa_plan_s *P, LaunchArgs a, const int64_t *items, int64_t c
     a.scratch_s = P->scratch_s.ptr;
     a.scratch_stride = P->scratch_stride;
     a.num_slots = P->scratch_slots;
-    if (persistent && !shared_stream) {
-        B200SA_CUDA(cudaMemsetAsync(P->qhead.ptr, 0, sizeof(unsigned long long), st));
-        a.queue_head = P->qhead.ptr;
-    }
-    B200SA_CUDA(launch_sa(a, s.grid, s.warps_per_cta, s.region, st));
+    a.queue_head = (persistent && !shared_stream) ? qhead : nullptr;
+    B200SA_CUDA(launch_sa(s.variant, a, s.grid, s.warps_per_cta, s.region, st));
     return B200SA_OK;
 }
 
@@ -240,8 +302,7 @@ int collect_stats(b200sa_plan_s *P, const std::vector<std::pair<int, int>> &rang
                                cudaMemcpyDeviceToHost));
     for (auto &pr : ranges) {
         const int p = pr.first;
-        const int64_t att_per_read =
-            (int64_t)P->n[p] * P->sweeps[p];  // sweeps = sweeps_per_beta * num_betas
+        const int64_t att_per_read = (int64_t)P->n[p] * P->sweeps[p];
         for (int r = 0; r < pr.second; ++r) {
             const ReadStats &x = hs[(size_t)(P->read_off[p] + r)];
             stats->flips += (int64_t)x.flips;
@@ -254,11 +315,62 @@ int collect_stats(b200sa_plan_s *P, const std::vector<std::pair<int, int>> &rang
     return B200SA_OK;
 }
 
+// Persistent mode: one launch per non-empty bucket, spread over forked
+// streams, the bucket with the longest items first so later buckets fill SMs
+// as earlier ones drain.
+int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
+                   size_t errlen) {
+    B200SA_CUDA(cudaMemsetAsync(P->qhead.ptr, 0, sizeof(unsigned long long) * kBuckets, st));
+    B200SA_CUDA(cudaEventRecord(P->fork, st));
+    int order[kBuckets];
+    for (int b = 0; b < kBuckets; ++b) order[b] = b;
+    std::stable_sort(order, order + kBuckets, [&](int x, int y) {
+        return P->bucket_lead_cost[x] > P->bucket_lead_cost[y];
+    });
+    bool used[kStreams] = {};
+    int next = 0;
+    for (int i = 0; i < kBuckets; ++i) {
+        const int b = order[i];
+        const int64_t cnt = P->bucket_off[b + 1] - P->bucket_off[b];
+        if (cnt <= 0) continue;
+        const int si = next++ % kStreams;
+        if (!used[si]) B200SA_CUDA(cudaStreamWaitEvent(P->bstream[si], P->fork, 0));
+        used[si] = true;
+        int rc = launch_items(P, a, b % kKinds, P->items_lpt.ptr + P->bucket_off[b], cnt,
+                              P->bucket_max_n[b], true, false, P->qhead.ptr + b,
+                              P->bstream[si], err, errlen);
+        if (rc) return rc;
+    }
+    for (int si = 0; si < kStreams; ++si) {
+        if (!used[si]) continue;
+        B200SA_CUDA(cudaEventRecord(P->join[si], P->bstream[si]));
+        B200SA_CUDA(cudaStreamWaitEvent(st, P->join[si], 0));
+    }
+    return B200SA_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
-const char *b200sa_version(void) { return "b200sa 0.1.0 (sm_100a)"; }
+const char *b200sa_version(void) { return "b200sa 0.3.0 (sm_100a)"; }
+
+int b200sa_check_acceptance(int64_t samples, uint64_t seed, int32_t device,
+                            int64_t counts[6], char *err, size_t errlen) {
+    if (!counts || samples < 0) return set_err(err, errlen, B200SA_EINVAL, "bad arguments");
+    DeviceGuard guard;
+    cudaDeviceProp prop;
+    int rc = select_device(device, prop, err, errlen);
+    if (rc) return rc;
+    DevArray<unsigned long long> d;
+    B200SA_CUDA(d.alloc(6));
+    B200SA_CUDA(cudaMemset(d.ptr, 0, 6 * sizeof(unsigned long long)));
+    B200SA_CUDA(acceptance_check(samples, seed, d.ptr));
+    unsigned long long h[6];
+    B200SA_CUDA(cudaMemcpy(h, d.ptr, sizeof(h), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < 6; ++i) counts[i] = (int64_t)h[i];
+    return B200SA_OK;
+}
 
 int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
                        int32_t device, b200sa_plan *out, char *err, size_t errlen) {
@@ -280,14 +392,29 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
     if (rc) return rc;
     P->device = device;
     B200SA_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+    for (int b = 0; b < kStreams; ++b) {
+        B200SA_CUDA(cudaStreamCreateWithFlags(&P->bstream[b], cudaStreamNonBlocking));
+        B200SA_CUDA(cudaEventCreateWithFlags(&P->join[b], cudaEventDisableTiming));
+    }
     B200SA_CUDA(cudaEventCreate(&P->ev0));
     B200SA_CUDA(cudaEventCreate(&P->ev1));
+    B200SA_CUDA(cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming));
     P->num_problems = num_problems;
+    // On chip when at least three warps' regions fit in one SM.
+    {
+        const int smem_sm = (int)P->prop.sharedMemPerMultiprocessor;
+        int lo = 0, hi = 1 << 20;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (3 * region_bytes_for(mid) + 3 * 1024 <= smem_sm) lo = mid; else hi = mid - 1;
+        }
+        P->onchip_max = lo;
+    }
 
     // Pack and lay out every problem in one device arena.
     std::vector<PackedAdjacency> adj((size_t)num_problems);
     struct Off {
-        size_t row, col, w, h, vinfo, cu, cv, cw, betas, thr;
+        size_t vinfo, dist, share, col, w, h, cu, cv, cw, betas, thr;
     };
     std::vector<Off> off((size_t)num_problems);
     size_t bytes = 0;
@@ -304,11 +431,12 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         const size_t n = (size_t)q.num_vars, m = (size_t)q.num_couplers,
                      nb = (size_t)q.num_betas;
         Off &o = off[i];
-        o.row = take(4 * (n + 1));
+        o.vinfo = take(8 * n);
+        o.dist = take(n);
+        o.share = take(4 * n);
         o.col = take(4 * 2 * m);
         o.w = take(8 * 2 * m);
         o.h = take(8 * n);
-        o.vinfo = take(n);
         o.cu = take(4 * m);
         o.cv = take(4 * m);
         o.cw = take(8 * m);
@@ -329,7 +457,6 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         const Off &o = off[i];
         const size_t n = (size_t)q.num_vars, m = (size_t)q.num_couplers,
                      nb = (size_t)q.num_betas;
-        std::memcpy(&staging[o.row], adj[i].row.data(), 4 * (n + 1));
         if (m) {
             std::memcpy(&staging[o.col], adj[i].col.data(), 4 * 2 * m);
             std::memcpy(&staging[o.w], adj[i].w.data(), 8 * 2 * m);
@@ -338,8 +465,11 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
             std::memcpy(&staging[o.cw], q.coupler_weights, 8 * m);
         }
         if (n) {
+            std::memcpy(&staging[o.vinfo], adj[i].vinfo.data(), 8 * n);
+            for (size_t v = 0; v < n; ++v)
+                staging[o.dist + v] = (uint8_t)(adj[i].vinfo[2 * v + 1] >> kDistShift);
+            std::memcpy(&staging[o.share], adj[i].share.data(), 4 * n);
             std::memcpy(&staging[o.h], q.h, 8 * n);
-            std::memcpy(&staging[o.vinfo], adj[i].vinfo.data(), n);
         }
         if (nb) {
             std::memcpy(&staging[o.betas], q.beta_schedule, 8 * nb);
@@ -365,11 +495,12 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         d.m = q.num_couplers;
         d.state_offset = P->state_off[i];
         d.read_offset = P->read_off[i];
-        d.row = reinterpret_cast<const int32_t *>(base + o.row);
+        d.vinfo = reinterpret_cast<const uint2 *>(base + o.vinfo);
+        d.dist = base + o.dist;
+        d.share = reinterpret_cast<const uint32_t *>(base + o.share);
         d.col = reinterpret_cast<const int32_t *>(base + o.col);
         d.w = reinterpret_cast<const double *>(base + o.w);
         d.h = reinterpret_cast<const double *>(base + o.h);
-        d.vinfo = base + o.vinfo;
         d.cu = reinterpret_cast<const int32_t *>(base + o.cu);
         d.cv = reinterpret_cast<const int32_t *>(base + o.cv);
         d.cw = reinterpret_cast<const double *>(base + o.cw);
@@ -377,6 +508,10 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         d.thresholds = reinterpret_cast<const double *>(base + o.thr);
         d.varorder = q.varorder;
         d.proposal = q.proposal;
+        d.regular_degree = adj[i].regular_degree;
+        d.regular_magic = d.regular_degree ? (65536u + (uint32_t)d.regular_degree - 1) /
+                                                 (uint32_t)d.regular_degree
+                                           : 0u;
     }
     B200SA_CUDA(P->dprobs.alloc((size_t)std::max(num_problems, 1)));
     if (num_problems)
@@ -384,9 +519,10 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
                                     sizeof(ProblemDev) * (size_t)num_problems,
                                     cudaMemcpyHostToDevice, P->stream));
 
-    // Seeds and work items.
+    // Seeds and work items: plain order (problem, read) and, for the
+    // persistent mode, grouped by size bucket, longest first inside a bucket.
     std::vector<uint64_t> seeds((size_t)P->total_reads);
-    std::vector<int64_t> plain, lpt;
+    std::vector<int64_t> plain;
     plain.reserve((size_t)P->total_reads);
     P->plain_item_off.assign((size_t)num_problems + 1, 0);
     for (int32_t i = 0; i < num_problems; ++i) {
@@ -399,19 +535,35 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         }
     }
     P->plain_item_off[num_problems] = (int64_t)plain.size();
-    lpt = plain;
-    // Longest work first so the tail of a persistent launch is short.
-    std::stable_sort(lpt.begin(), lpt.end(), [&](int64_t a, int64_t b) {
-        const int pa = (int)(a >> 32), pb = (int)(b >> 32);
-        const int64_t ca = (int64_t)P->n[pa] * P->sweeps[pa];
-        const int64_t cb = (int64_t)P->n[pb] * P->sweeps[pb];
-        return ca > cb;
+    auto cost = [&](int64_t it) {
+        const int p = (int)(it >> 32);
+        return (int64_t)P->n[p] * P->sweeps[p];
+    };
+    auto bucket_of = [&](int64_t it) {
+        const int p = (int)(it >> 32);
+        return size_class(P->n[p], P->onchip_max) * kKinds + kind_of(P->hprobs[p]);
+    };
+    std::vector<int64_t> lpt = plain;
+    std::stable_sort(lpt.begin(), lpt.end(), [&](int64_t x, int64_t y) {
+        const int bx = bucket_of(x), by = bucket_of(y);
+        if (bx != by) return bx < by;
+        return cost(x) > cost(y);
     });
+    for (int b = 0; b <= kBuckets; ++b) P->bucket_off[b] = 0;
+    for (int64_t it : lpt) {
+        const int p = (int)(it >> 32);
+        const int b = bucket_of(it);
+        P->bucket_off[b + 1]++;
+        P->bucket_max_n[b] = std::max(P->bucket_max_n[b], P->n[p]);
+        P->bucket_lead_cost[b] = std::max(P->bucket_lead_cost[b], cost(it));
+    }
+    for (int b = 0; b < kBuckets; ++b) P->bucket_off[b + 1] += P->bucket_off[b];
+
     B200SA_CUDA(P->dseeds.alloc(std::max<size_t>(seeds.size(), 1)));
     B200SA_CUDA(P->dstats.alloc(std::max<size_t>(seeds.size(), 1)));
     B200SA_CUDA(P->items_plain.alloc(std::max<size_t>(plain.size(), 1)));
     B200SA_CUDA(P->items_lpt.alloc(std::max<size_t>(lpt.size(), 1)));
-    B200SA_CUDA(P->qhead.alloc(1));
+    B200SA_CUDA(P->qhead.alloc(kBuckets));
     if (!seeds.empty())
         B200SA_CUDA(cudaMemcpyAsync(P->dseeds.ptr, seeds.data(), 8 * seeds.size(),
                                     cudaMemcpyHostToDevice, P->stream));
@@ -421,7 +573,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         B200SA_CUDA(cudaMemcpyAsync(P->items_lpt.ptr, lpt.data(), 8 * lpt.size(),
                                     cudaMemcpyHostToDevice, P->stream));
     }
-    B200SA_CUDA(upload_jump_columns(jump_columns(), P->stream));
+    B200SA_CUDA(upload_jump_table(jump_table(), P->stream));
     B200SA_CUDA(cudaStreamSynchronize(P->stream));
     *out = P.release();
     return B200SA_OK;
@@ -440,7 +592,7 @@ int b200sa_plan_destroy(b200sa_plan plan) {
     if (!plan) return B200SA_OK;
     DeviceGuard guard;
     cudaSetDevice(plan->device);
-    cudaStreamSynchronize(plan->stream);
+    cudaDeviceSynchronize();
     delete plan;
     return B200SA_OK;
 }
@@ -468,15 +620,13 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
     B200SA_CUDA(cudaEventRecord(plan->ev0, st));
     int rc = B200SA_OK;
     if (mode == B200SA_MODE_PERSISTENT) {
-        rc = launch_items(plan, a, plan->items_lpt.ptr,
-                          plan->plain_item_off[plan->num_problems], plan->max_n, true,
-                          false, st, err, errlen);
+        rc = run_persistent(plan, a, st, err, errlen);
     } else {
         for (int i = 0; i < plan->num_problems && rc == B200SA_OK; ++i) {
             const int64_t o = plan->plain_item_off[i];
-            rc = launch_items(plan, a, plan->items_plain.ptr + o,
+            rc = launch_items(plan, a, kind_of(plan->hprobs[i]), plan->items_plain.ptr + o,
                               plan->plain_item_off[i + 1] - o, plan->n[i], false, false,
-                              st, err, errlen);
+                              nullptr, st, err, errlen);
         }
     }
     if (rc) return rc;
@@ -501,6 +651,15 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
 
 int b200sa_sample_batch(const b200sa_problem *problems, int32_t num_problems, int32_t mode,
                         int32_t device, b200sa_stats *stats, char *err, size_t errlen) {
+    for (int i = 0; i < num_problems && problems; ++i) {
+        const size_t sz = (size_t)problems[i].num_reads * (size_t)problems[i].num_vars;
+        if (sz && !problems[i].states)
+            return set_err(err, errlen, B200SA_EINVAL,
+                           "problem " + std::to_string(i) + ": states is NULL");
+        if (problems[i].num_reads > 0 && !problems[i].energies)
+            return set_err(err, errlen, B200SA_EINVAL,
+                           "problem " + std::to_string(i) + ": energies is NULL");
+    }
     b200sa_plan plan = nullptr;
     int rc = b200sa_plan_create(problems, num_problems, device, &plan, err, errlen);
     if (rc) return rc;
@@ -513,16 +672,9 @@ int b200sa_sample_batch(const b200sa_problem *problems, int32_t num_problems, in
     B200SA_CUDA(den.alloc((size_t)std::max<int64_t>(plan->total_reads, 1)));
     for (int i = 0; i < num_problems; ++i) {
         const size_t sz = (size_t)problems[i].num_reads * (size_t)problems[i].num_vars;
-        if (sz) {
-            if (!problems[i].states)
-                return set_err(err, errlen, B200SA_EINVAL,
-                               "problem " + std::to_string(i) + ": states is NULL");
+        if (sz)
             B200SA_CUDA(cudaMemcpyAsync(dstates.ptr + plan->state_off[i], problems[i].states,
                                         sz, cudaMemcpyHostToDevice, plan->stream));
-        }
-        if (problems[i].num_reads > 0 && !problems[i].energies)
-            return set_err(err, errlen, B200SA_EINVAL,
-                           "problem " + std::to_string(i) + ": energies is NULL");
     }
     rc = b200sa_plan_run(plan, mode, dstates.ptr, dstates.ptr, den.ptr, nullptr, nullptr, 1,
                          stats, err, errlen);
@@ -559,8 +711,6 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
         return set_err(err, errlen, B200SA_EINVAL,
                        "num_seeds must be 1 (one continued stream) or num_reads (per read)");
     const bool shared = num_seeds == 1 && num_reads > 1;
-    std::vector<uint64_t> per_read;
-    if (num_seeds == 1 && !shared) per_read.assign(1, seeds[0]);
     b200sa_problem q{};
     q.num_vars = num_vars;
     q.h = h;
@@ -579,7 +729,7 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
         shared_seeds.assign((size_t)num_reads, seeds[0]);
         q.seeds = shared_seeds.data();
     } else {
-        q.seeds = per_read.empty() ? seeds : per_read.data();
+        q.seeds = seeds;
     }
     q.varorder = varorder;
     q.proposal = proposal;
@@ -621,12 +771,14 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
             chunk = 1;
         } else {
             LaunchShape s{};
-            rc = shape_for(plan, num_vars, num_reads, true, s, err, errlen);
+            rc = shape_for(plan, kind_of(plan->hprobs[0]), num_vars, num_reads, true, s, err,
+                           errlen);
             if (rc) return rc;
-            int per_sm = 0;
-            B200SA_CUDA(kernel_occupancy(s.warps_per_cta, s.region, &per_sm));
+            int ctas = 0;
+            rc = occupancy(plan, s.variant, s.warps_per_cta, s.region, &ctas, err, errlen);
+            if (rc) return rc;
             chunk = std::max<int64_t>(
-                1, (int64_t)plan->prop.multiProcessorCount * per_sm * s.warps_per_cta);
+                1, (int64_t)plan->prop.multiProcessorCount * ctas * s.warps_per_cta);
         }
     }
     LaunchArgs a = base_args(plan, dstates.ptr, dstates.ptr, den.ptr, nullptr);
@@ -638,9 +790,11 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
     while (done < num_reads && !stop) {
         const int64_t cnt = std::min<int64_t>(chunk, num_reads - done);
         a.carry_in = (shared && done > 0) ? 1 : 0;
+        B200SA_CUDA(cudaMemsetAsync(plan->qhead.ptr, 0, sizeof(unsigned long long),
+                                    plan->stream));
         B200SA_CUDA(cudaEventRecord(plan->ev0, plan->stream));
-        rc = launch_items(plan, a, plan->items_plain.ptr + done, cnt, num_vars, !shared,
-                          shared, plan->stream, err, errlen);
+        rc = launch_items(plan, a, kind_of(plan->hprobs[0]), plan->items_plain.ptr + done, cnt,
+                          num_vars, !shared, shared, plan->qhead.ptr, plan->stream, err, errlen);
         if (rc) return rc;
         B200SA_CUDA(cudaEventRecord(plan->ev1, plan->stream));
         B200SA_CUDA(cudaStreamSynchronize(plan->stream));

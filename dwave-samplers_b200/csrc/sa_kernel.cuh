@@ -19,10 +19,17 @@
 // neighbour, so the pass commits the prefix of lanes before the smallest such
 // bound.  The committed prefix is exactly what the reference computes
 // one variable at a time: its delta energies were untouched by earlier flips
-// in the window and its draws land on the same stream positions.  Committed
-// flips are pairwise non-adjacent; their neighbour updates are applied flip
-// by flip in variable order, so additions into a shared neighbour keep the
-// reference's order.
+// in the window and its draws land on the same stream positions.
+//
+// Committed flips are pairwise non-adjacent, so their neighbour updates never
+// touch each other's slots or spins.  They are applied together: the
+// adjacency entries of all committed flips, concatenated in variable order,
+// are spread over the lanes 32 at a time.  Entries that name the same slot
+// (a neighbour shared by two flips, or a self-loop / repeated coupler) are
+// grouped with __match_any_sync and summed by the group's first lane in
+// entry order, so every slot receives its additions in the reference's order.
+// The grouping is skipped when the per-variable conflict masks (computed at
+// pack time) show that no two entries of the pass can name the same slot.
 #pragma once
 #include <cstdint>
 
@@ -30,7 +37,8 @@
 
 namespace b200sa {
 
-__constant__ uint4 c_jump[128];  // xorshift128+ advanced by kHalf steps
+// Nibble tables of the GF(2) matrix (xorshift128+ transition)^kHalf.
+__device__ uint4 g_jump_nib[kJumpTable];
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr double kTwo64 = 18446744073709551616.0;  // (double)RANDMAX
@@ -50,6 +58,109 @@ struct Counters {
     unsigned int near;
 };
 
+// ---- acceptance tests ------------------------------------------------------
+// The reference decides Metropolis as exp(x) * 2^64 > (double)rand with
+// x = -dE*beta (cpu_sa.cpp:154) and Gibbs as 2^64 > (double)rand * (1 +
+// exp(z)) with z = dE*beta (cpu_sa.cpp:163).  Both are first decided in the
+// log2 domain with single-precision hardware approximations, whose total
+// error is below 2^-14 in log2 units for the argument ranges that reach them
+// (|x| < 44.4 and z < 44.4 since dE < 44.36142/beta): every term's error is
+// bounded by a few single-precision roundings of magnitudes <= 110 plus the
+// lg2/ex2 approximation error (relative 2^-22).  When the two sides differ by
+// more than kBand = 2^-10 the fast answer equals the exact one; otherwise the
+// exact double-precision expression is evaluated.  The band is reached by
+// about 0.1% of draws.
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kBand = 0.0009765625f;  // 2^-10
+
+__device__ __forceinline__ float lg2_approx(float x) {
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float ex2_approx(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// 1 accept, 0 reject, -1 undecided.  x = -dE*beta in (-44.4, 0].
+__device__ __forceinline__ int metropolis_fast(double x, uint64_t r) {
+    const float t = __fmaf_rn((float)x, kLog2e, 64.0f);  // log2(exp(x) * 2^64)
+    const float y = lg2_approx(__ull2float_rn(r));      // log2(rand); -inf at 0
+    if (t > y + kBand) return 1;
+    if (t < y - kBand) return 0;
+    return -1;
+}
+
+// 1 accept, 0 reject, -1 undecided.  z = dE*beta < 44.4 (may be -inf).
+__device__ __forceinline__ int gibbs_fast(double z, uint64_t r) {
+    const float zf = (float)z;
+    float g;  // log2(1 + exp(z))
+    if (zf > 24.0f)
+        g = zf * kLog2e;  // log2(1 + exp(-z)) < 2^-33 omitted
+    else if (zf < -24.0f)
+        g = 0.0f;  // log2(1 + exp(z)) < 2^-33
+    else
+        g = lg2_approx(1.0f + ex2_approx(zf * kLog2e));
+    const float s = lg2_approx(__ull2float_rn(r)) + g;  // log2(rand * (1 + exp(z)))
+    if (s < 64.0f - kBand) return 1;
+    if (s > 64.0f + kBand) return 0;
+    return -1;
+}
+
+// The exact double-precision decisions, reached only inside the band.  Kept
+// out of line so the sweep loop does not hold exp()'s registers.
+// Returns accept in bit 0 and the near-tie flag in bit 1.
+__device__ __noinline__ int metropolis_exact(double d, double beta, uint64_t r) {
+    const double rd = __ull2double_rn(r);
+    const double e = exp(__dmul_rn(-d, beta));  // cpu_sa.cpp:152-154
+    const double x = __dmul_rn(e, kTwo64);
+    return (x > rd ? 1 : 0) | (fabs(x - rd) <= x * kTieRel ? 2 : 0);
+}
+
+__device__ __noinline__ int gibbs_exact(double d, double beta, uint64_t r) {
+    const double rd = __ull2double_rn(r);
+    const double e = exp(__dmul_rn(d, beta));  // cpu_sa.cpp:162-163
+    const double y = __dmul_rn(rd, __dadd_rn(1.0, e));
+    return (kTwo64 > y ? 1 : 0) | (fabs(y - kTwo64) <= kTwo64 * kTieRel ? 2 : 0);
+}
+
+// Problem fields the sweep loop keeps in registers (fields used only when a
+// read starts or ends are read from the ProblemDev record there).
+struct Prob {
+    int n;
+    int sweeps_per_beta;
+    int num_betas;
+    const uint2 *__restrict__ vinfo;
+    const int32_t *__restrict__ col;
+    const double *__restrict__ w;
+    const double *__restrict__ betas;
+    const double *__restrict__ thresholds;
+    const uint8_t *__restrict__ dist;
+    const uint32_t *__restrict__ share;
+    int regular_degree;
+    uint32_t regular_magic;
+};
+
+__device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
+    Prob q;
+    q.n = P->n;
+    q.sweeps_per_beta = P->sweeps_per_beta;
+    q.num_betas = P->num_betas;
+    q.vinfo = P->vinfo;
+    q.col = P->col;
+    q.w = P->w;
+    q.betas = P->betas;
+    q.thresholds = P->thresholds;
+    q.dist = P->dist;
+    q.share = P->share;
+    q.regular_degree = P->regular_degree;
+    q.regular_magic = P->regular_magic;
+    return q;
+}
+
 __device__ __forceinline__ void xs_advance(uint64_t &s0, uint64_t &s1) {
     uint64_t a = s0;
     const uint64_t b = s1;
@@ -64,24 +175,19 @@ __device__ __forceinline__ uint64_t xs_next(uint64_t &s0, uint64_t &s1) {
     return s1 + b;
 }
 
-// State <- M * state over GF(2), M = (xorshift128+ transition)^kHalf given by
-// its columns in constant memory (every lane reads the same column: broadcast).
-// The column loop is only partly unrolled so the 128 column loads stay inside
-// it instead of being hoisted into registers by the callers' loops.
+// State <- M * state over GF(2), M = (xorshift128+ transition)^kHalf: the
+// XOR of one table entry per nibble of the 128-bit state (32 lookups).
 __device__ __forceinline__ void xs_jump(uint64_t &s0, uint64_t &s1) {
     uint32_t a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll 1
-    for (int k = 0; k < 4; ++k) {
-        const uint32_t w = (uint32_t)((k < 2 ? s0 : s1) >> ((k & 1) * 32));
-#pragma unroll 8
-        for (int b = 0; b < 32; ++b) {
-            const uint32_t mk = 0u - ((w >> b) & 1u);
-            const uint4 c = c_jump[k * 32 + b];
-            a0 ^= c.x & mk;
-            a1 ^= c.y & mk;
-            a2 ^= c.z & mk;
-            a3 ^= c.w & mk;
-        }
+#pragma unroll
+    for (int k = 0; k < kJumpNibbles; ++k) {
+        const uint64_t word = k < 16 ? s0 : s1;
+        const uint32_t nib = (uint32_t)(word >> (4 * (k & 15))) & 15u;
+        const uint4 c = __ldg(&g_jump_nib[k * 16 + nib]);
+        a0 ^= c.x;
+        a1 ^= c.y;
+        a2 ^= c.z;
+        a3 ^= c.w;
     }
     s0 = (uint64_t)a0 | ((uint64_t)a1 << 32);
     s1 = (uint64_t)a2 | ((uint64_t)a3 << 32);
@@ -114,61 +220,195 @@ __device__ __forceinline__ void ring_init(uint64_t *ring, RingState &rs,
     __syncwarp();
 }
 
+// Overwrites the consumed lower half with the positions kRing further on and
+// returns this lane's next segment-start state.  Out of line: it runs once per
+// kHalf draws.
+__device__ __noinline__ ulonglong2 ring_refill_half(uint64_t *ring, uint64_t pos,
+                                                    ulonglong2 t, unsigned lane) {
+    __syncwarp();
+    ring_fill(ring, pos, t.x, t.y, lane);
+    uint64_t s0 = t.x, s1 = t.y;
+    xs_jump(s0, s1);
+    __syncwarp();
+    return make_ulonglong2(s0, s1);
+}
+
 // Keeps positions [q, q + kHalf) available: once the lower half is consumed
 // it is overwritten with the positions kRing further on.
 __device__ __forceinline__ void ring_refill(uint64_t *ring, RingState &rs,
                                             unsigned lane) {
     if (rs.q - rs.base >= (uint64_t)kHalf) {
-        __syncwarp();
-        ring_fill(ring, rs.base + kRing, rs.t0, rs.t1, lane);
-        xs_jump(rs.t0, rs.t1);
+        const ulonglong2 t =
+            ring_refill_half(ring, rs.base + kRing, make_ulonglong2(rs.t0, rs.t1), lane);
+        rs.t0 = t.x;
+        rs.t1 = t.y;
         rs.base += kHalf;
-        __syncwarp();
     }
 }
 
 // cpu_sa.cpp:54-74 for every variable, then the working copy of the spins.
-__device__ __forceinline__ void load_state(const ProblemDev &P,
-                                           const int8_t *src, double *de,
-                                           int8_t *sp, unsigned lane) {
-    const int n = P.n;
+__device__ __forceinline__ void load_state(const ProblemDev *PD, const int8_t *src,
+                                           double *de, int8_t *sp,
+                                           unsigned lane) {
+    const int n = PD->n;
+    const uint2 *__restrict__ vinfo = PD->vinfo;
+    const int32_t *__restrict__ col = PD->col;
+    const double *__restrict__ w = PD->w;
+    const double *__restrict__ h = PD->h;
     for (int v = lane; v < n; v += 32) sp[v] = src[v];
     __syncwarp();
     for (int v = lane; v < n; v += 32) {
-        double f = __ldg(&P.h[v]);
-        const int e1 = __ldg(&P.row[v + 1]);
-        for (int e = __ldg(&P.row[v]); e < e1; ++e)
-            f = __dadd_rn(f, __dmul_rn((double)(int)sp[__ldg(&P.col[e])],
-                                       __ldg(&P.w[e])));
+        const uint2 vi = __ldg(&vinfo[v]);
+        const int e1 = (int)vi.x + (int)(vi.y & kDegMask);
+        double f = __ldg(&h[v]);
+        for (int e = (int)vi.x; e < e1; ++e)
+            f = __dadd_rn(f, __dmul_rn((double)(int)sp[__ldg(&col[e])], __ldg(&w[e])));
         de[v] = __dmul_rn((double)(-2 * (int)sp[v]), f);
     }
     __syncwarp();
 }
 
-// cpu_sa.cpp:168-191 for variable v.  Distinct neighbour slots are updated
-// lane-parallel; a list with repeated targets runs on one lane in order.
-__device__ __forceinline__ void apply_flip(const ProblemDev &P, double *de,
-                                           int8_t *sp, int v, unsigned lane) {
-    const int s_old = sp[v];
+// cpu_sa.cpp:168-191 for every lane whose bit is set in `fm`.  Lane k of
+// the warp holds its variable v, list start `start`, degree `deg` and spin
+// `s_old` (valid on flipping lanes).  The flipping variables must be pairwise
+// non-adjacent.  Entries are applied lane-parallel in rounds of 32; equal
+// targets within a round are summed in entry order by their first lane.
+// `scratch` holds 32 doubles followed by 32 ints.
+__device__ __forceinline__ void apply_flips(const Prob &P, double *de, int8_t *sp,
+                                            double *scratch, unsigned fm, int v,
+                                            int start, int deg, int s_old,
+                                            bool may_conflict, unsigned lane) {
+    const bool f = (fm >> lane) & 1u;
     const double mult = (double)(int)(int8_t)(4 * s_old);
-    const int e0 = __ldg(&P.row[v]), e1 = __ldg(&P.row[v + 1]);
-    if (!(__ldg(&P.vinfo[v]) & kDupFlag)) {
-        for (int e = e0 + (int)lane; e < e1; e += 32) {
-            const int nb = __ldg(&P.col[e]);
-            const double upd = __dmul_rn(__dmul_rn(mult, __ldg(&P.w[e])),
-                                         (double)(int)sp[nb]);
-            de[nb] = __dadd_rn(de[nb], upd);
+    int *owner_of_rank = reinterpret_cast<int *>(scratch + 32);
+    const int D = P.regular_degree;
+    int excl = 0, total;
+    if (D) {
+        // Equal list lengths: entry t belongs to the (t / D)-th flip.
+        if (f) owner_of_rank[__popc(fm & ((1u << lane) - 1u))] = (int)lane;
+        total = __popc(fm) * D;
+        __syncwarp();
+    } else {
+        const int my = f ? deg : 0;
+        int incl = my;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(kFull, incl, o);
+            if ((int)lane >= o) incl += y;
         }
-    } else if (lane == 0) {
-        for (int e = e0; e < e1; ++e) {
-            const int nb = __ldg(&P.col[e]);
-            const double upd = __dmul_rn(__dmul_rn(mult, __ldg(&P.w[e])),
-                                         (double)(int)sp[nb]);
-            de[nb] = __dadd_rn(de[nb], upd);
+        excl = incl - my;
+        total = __shfl_sync(kFull, incl, 31);
+    }
+    for (int base = 0; base < total; base += 32) {
+        const int t = base + (int)lane;
+        const bool a = t < total;
+        int k, e;
+        if (D) {
+            const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);  // t / D
+            k = a ? owner_of_rank[r] : 0;
+            e = __shfl_sync(kFull, v, k) * D + (t - r * D);
+        } else {
+            // Owner: the last lane whose entry range starts at or before t.
+            k = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const int ex = __shfl_sync(kFull, excl, k + step);
+                if (ex <= t) k += step;
+            }
+            e = __shfl_sync(kFull, start, k) + (t - __shfl_sync(kFull, excl, k));
         }
+        const double m_k = __shfl_sync(kFull, mult, k);
+        int nb = -1 - (int)lane;  // distinct per inactive lane
+        double x = 0.0;
+        if (a) {
+            nb = __ldg(&P.col[e]);
+            x = __dmul_rn(__dmul_rn(m_k, __ldg(&P.w[e])), (double)(int)sp[nb]);
+        }
+        const unsigned grp = may_conflict ? __match_any_sync(kFull, nb) : (1u << lane);
+        const bool alone = grp == (1u << lane);
+        if (a && alone) de[nb] = __dadd_rn(de[nb], x);
+        if (may_conflict && __any_sync(kFull, a && !alone)) {
+            scratch[lane] = x;
+            __syncwarp();
+            if (a && !alone && lane == (unsigned)(__ffs(grp) - 1)) {
+                double acc = de[nb];
+                unsigned g = grp;
+                while (g) {
+                    const int j = __ffs(g) - 1;
+                    g &= g - 1;
+                    acc = __dadd_rn(acc, scratch[j]);
+                }
+                de[nb] = acc;
+            }
+        }
+        __syncwarp();
+    }
+    if (f) {  // cpu_sa.cpp:189-190, after the variable's own updates
+        sp[v] = (int8_t)(-s_old);
+        de[v] = __dmul_rn(de[v], -1.0);
     }
     __syncwarp();
-    if (lane == 0) {
+}
+
+// Neighbour updates of the committed flips `fm` for equal-length lists (D
+// entries each, list v at v * D).  The entries of the first 64 accepted flips
+// were loaded into (nb0, w0, k0) / (nb1, w1, k1) before the commit was known
+// (the committed flips are a prefix of the accepted ones, in lane order);
+// later entries are loaded here.  Same grouping rule as apply_flips.
+__device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t *sp,
+                                               double *scratch, const int *owner_of_rank,
+                                               unsigned fm, int p, int v, int s_old,
+                                               int nb0, double w0, int k0, int nb1,
+                                               double w1, int k1, bool may_conflict,
+                                               unsigned lane) {
+    const int D = P.regular_degree;
+    const double mult = (double)(int)(int8_t)(4 * s_old);
+    const int total = __popc(fm) * D;
+    for (int base = 0; base < total; base += 32) {
+        const int t = base + (int)lane;
+        const bool a = t < total;
+        int k, nb;
+        double wt;
+        if (base == 0) {
+            k = k0, nb = nb0, wt = w0;
+        } else if (base == 32) {
+            k = k1, nb = nb1, wt = w1;
+        } else {
+            k = 0, nb = 0, wt = 0.0;
+            if (a) {
+                const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
+                k = owner_of_rank[r];
+                const int e = (p + k) * D + (t - r * D);
+                nb = __ldg(&P.col[e]);
+                wt = __ldg(&P.w[e]);
+            }
+        }
+        const double m_k = __shfl_sync(kFull, mult, k);
+        double x = 0.0;
+        if (a)
+            x = __dmul_rn(__dmul_rn(m_k, wt), (double)(int)sp[nb]);
+        else
+            nb = -1 - (int)lane;  // distinct per inactive lane
+        const unsigned grp = may_conflict ? __match_any_sync(kFull, nb) : (1u << lane);
+        const bool alone = grp == (1u << lane);
+        if (a && alone) de[nb] = __dadd_rn(de[nb], x);
+        if (may_conflict && __any_sync(kFull, a && !alone)) {
+            scratch[lane] = x;
+            __syncwarp();
+            if (a && !alone && lane == (unsigned)(__ffs(grp) - 1)) {
+                double acc = de[nb];
+                unsigned g = grp;
+                while (g) {
+                    const int j = __ffs(g) - 1;
+                    g &= g - 1;
+                    acc = __dadd_rn(acc, scratch[j]);
+                }
+                de[nb] = acc;
+            }
+        }
+        __syncwarp();
+    }
+    if ((fm >> lane) & 1u) {  // cpu_sa.cpp:189-190, after the variable's own updates
         sp[v] = (int8_t)(-s_old);
         de[v] = __dmul_rn(de[v], -1.0);
     }
@@ -176,12 +416,14 @@ __device__ __forceinline__ void apply_flip(const ProblemDev &P, double *de,
 }
 
 template <bool GIBBS>
-__device__ __forceinline__ void sweep_sequential(const ProblemDev &P,
-                                                 double *de, int8_t *sp,
+__device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
+                                                 int8_t *sp, double *scratch,
                                                  uint64_t *ring, RingState &rs,
                                                  unsigned lane, Counters &cnt) {
     const int n = P.n;
+    const int D = P.regular_degree;
     const unsigned lt_mask = (1u << lane) - 1u;
+    int *owner_of_rank = reinterpret_cast<int *>(scratch + 32);
     for (int b = 0; b < P.num_betas; ++b) {
         const double beta = __ldg(&P.betas[b]);
         const double thr = __ldg(&P.thresholds[b]);
@@ -192,8 +434,16 @@ __device__ __forceinline__ void sweep_sequential(const ProblemDev &P,
                 const int L = min(32, n - p);
                 const int v = p + (int)lane;
                 const bool act = (int)lane < L;
-                const double d = act ? de[v] : 0.0;
-                const int dist = act ? (int)(__ldg(&P.vinfo[v]) & kDistMask) : 32;
+                double d = 0.0;
+                int dist = 32;
+                unsigned shr = 0u;
+                uint2 vi = make_uint2(0u, 0u);
+                if (act) {
+                    d = de[v];
+                    dist = __ldg(&P.dist[v]);
+                    shr = __ldg(&P.share[v]);
+                    if (!D) vi = __ldg(&P.vinfo[v]);
+                }
                 const bool consider = act && !(d >= thr);  // cpu_sa.cpp:140
                 const bool need = GIBBS ? consider : (consider && !(d <= 0.0));
                 const unsigned need_mask = __ballot_sync(kFull, need);
@@ -201,34 +451,64 @@ __device__ __forceinline__ void sweep_sequential(const ProblemDev &P,
                 bool near = false;
                 if (need) {
                     const uint64_t r =
-                        ring[(rs.q + (uint64_t)__popc(need_mask & lt_mask)) &
-                             (kRing - 1)];
-                    const double rd = __ull2double_rn(r);
-                    if (GIBBS) {  // cpu_sa.cpp:162-163
-                        const double e = exp(__dmul_rn(d, beta));
-                        const double y = __dmul_rn(rd, __dadd_rn(1.0, e));
-                        acc = kTwo64 > y;
-                        near = fabs(y - kTwo64) <= kTwo64 * kTieRel;
-                    } else {  // cpu_sa.cpp:152-154
-                        const double e = exp(__dmul_rn(-d, beta));
-                        const double x = __dmul_rn(e, kTwo64);
-                        acc = x > rd;
-                        near = fabs(x - rd) <= x * kTieRel;
+                        ring[(rs.q + (uint64_t)__popc(need_mask & lt_mask)) & (kRing - 1)];
+                    const int fast = GIBBS ? gibbs_fast(__dmul_rn(d, beta), r)
+                                           : metropolis_fast(__dmul_rn(-d, beta), r);
+                    if (fast >= 0) {
+                        acc = fast != 0;
+                    } else {
+                        const int ex = GIBBS ? gibbs_exact(d, beta, r) : metropolis_exact(d, beta, r);
+                        acc = (ex & 1) != 0;
+                        near = (ex & 2) != 0;
                     }
                 }
-                const unsigned flip_mask = __ballot_sync(kFull, acc);
+                const unsigned am = __ballot_sync(kFull, acc);
+                // Equal-length lists: start loading the accepted flips'
+                // adjacency before the commit point is known.
+                int nb0 = 0, nb1 = 0, k0 = 0, k1 = 0;
+                double w0 = 0.0, w1 = 0.0;
+                if (D && am) {
+                    if (acc) owner_of_rank[__popc(am & lt_mask)] = (int)lane;
+                    __syncwarp();
+                    const int pre = min(__popc(am) * D, 64);
+                    if ((int)lane < pre) {
+                        const int r = (int)((lane * P.regular_magic) >> 16);
+                        k0 = owner_of_rank[r];
+                        const int e = (p + k0) * D + ((int)lane - r * D);
+                        nb0 = __ldg(&P.col[e]);
+                        w0 = __ldg(&P.w[e]);
+                    }
+                    if ((int)lane + 32 < pre) {
+                        const int t = (int)lane + 32;
+                        const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
+                        k1 = owner_of_rank[r];
+                        const int e = (p + k1) * D + (t - r * D);
+                        nb1 = __ldg(&P.col[e]);
+                        w1 = __ldg(&P.w[e]);
+                    }
+                }
                 const int bound = acc ? (int)lane + dist : 32;
                 const int c = min(__reduce_min_sync(kFull, bound), L);
                 const unsigned commit = c >= 32 ? kFull : ((1u << c) - 1u);
                 rs.q += (uint64_t)__popc(need_mask & commit);
+                const unsigned fm = am & commit;
                 cnt.near += __popc(__ballot_sync(kFull, near) & commit);
-                unsigned fm = flip_mask & commit;
                 cnt.flips += __popc(fm);
                 cnt.passes += 1;
-                while (fm) {
-                    const int k = __ffs(fm) - 1;
-                    fm &= fm - 1;
-                    apply_flip(P, de, sp, p + k, lane);
+                if (fm) {
+                    const int s_old = act ? (int)sp[v] : 0;
+                    // A slot can receive two additions only through a repeated
+                    // target in one list or a neighbour common to two flips.
+                    const unsigned later = lane < 31 ? fm >> (lane + 1) : 0u;
+                    const bool f = (fm >> lane) & 1u;
+                    const bool may_conflict =
+                        __any_sync(kFull, f && ((shr & 1u) || ((shr >> 1) & later)));
+                    if (D)
+                        update_regular(P, de, sp, scratch, owner_of_rank, fm, p, v, s_old, nb0,
+                                       w0, k0, nb1, w1, k1, may_conflict, lane);
+                    else
+                        apply_flips(P, de, sp, scratch, fm, v, (int)vi.x,
+                                    (int)(vi.y & kDegMask), s_old, may_conflict, lane);
                 }
                 p += c;
             }
@@ -239,10 +519,10 @@ __device__ __forceinline__ void sweep_sequential(const ProblemDev &P,
 // cpu_sa.cpp:134-136: each attempt draws its variable as rand % n.  One
 // attempt per step, warp-uniform; lanes share the neighbour update.
 template <bool GIBBS>
-__device__ __forceinline__ void sweep_random(const ProblemDev &P, double *de,
-                                             int8_t *sp, uint64_t *ring,
-                                             RingState &rs, unsigned lane,
-                                             Counters &cnt) {
+__device__ __forceinline__ void sweep_random(const Prob &P, double *de,
+                                             int8_t *sp, double *scratch,
+                                             uint64_t *ring, RingState &rs,
+                                             unsigned lane, Counters &cnt) {
     const int n = P.n;
     for (int b = 0; b < P.num_betas; ++b) {
         const double beta = __ldg(&P.betas[b]);
@@ -273,79 +553,70 @@ __device__ __forceinline__ void sweep_random(const ProblemDev &P, double *de,
                     acc = x > rd;
                     cnt.near += fabs(x - rd) <= x * kTieRel;
                 }
-                __syncwarp();
                 if (acc) {
                     cnt.flips += 1;
-                    apply_flip(P, de, sp, var, lane);
+                    const uint2 vi = __ldg(&P.vinfo[var]);
+                    const int s_old = (int)sp[var];
+                    __syncwarp();
+                    apply_flips(P, de, sp, scratch, 1u, var, (int)vi.x,
+                                (int)(vi.y & kDegMask), s_old,
+                                (__ldg(&P.share[var]) & 1u) != 0u, lane);
                 }
             }
         }
     }
 }
 
-// cpu_sa.cpp:210-227.  Terms are formed lane-parallel (products are exact
-// roundings of the same operands); the running sum is strictly sequential.
-__device__ __forceinline__ double state_energy(const ProblemDev &P,
-                                               const int8_t *sp,
+// cpu_sa.cpp:210-227.  Terms are formed lane-parallel (each an exact
+// rounding of the same operands); the running sum is strictly sequential.
+__device__ __forceinline__ double state_energy(const ProblemDev *PD, const int8_t *sp,
                                                unsigned lane) {
+    const int n = PD->n;
+    const int64_t m = PD->m;
+    const double *__restrict__ h = PD->h;
+    const int32_t *__restrict__ cu = PD->cu;
+    const int32_t *__restrict__ cv = PD->cv;
+    const double *__restrict__ cw = PD->cw;
     double e = 0.0;
-    for (int base = 0; base < P.n; base += 32) {
+    for (int base = 0; base < n; base += 32) {
         const int v = base + (int)lane;
-        const double t =
-            v < P.n ? __dmul_rn((double)(int)sp[v], __ldg(&P.h[v])) : 0.0;
-        const int cnt = min(32, P.n - base);
+        const double t = v < n ? __dmul_rn((double)(int)sp[v], __ldg(&h[v])) : 0.0;
+        const int cnt = min(32, n - base);
         for (int j = 0; j < cnt; ++j) e = __dadd_rn(e, __shfl_sync(kFull, t, j));
     }
-    for (int64_t base = 0; base < P.m; base += 32) {
+    for (int64_t base = 0; base < m; base += 32) {
         const int64_t c = base + lane;
         double t = 0.0;
-        if (c < P.m)
-            t = __dmul_rn(__dmul_rn((double)(int)sp[__ldg(&P.cu[c])], __ldg(&P.cw[c])),
-                          (double)(int)sp[__ldg(&P.cv[c])]);
-        const int cnt = (int)min((int64_t)32, P.m - base);
+        if (c < m)
+            t = __dmul_rn(__dmul_rn((double)(int)sp[__ldg(&cu[c])], __ldg(&cw[c])),
+                          (double)(int)sp[__ldg(&cv[c])]);
+        const int cnt = (int)min((int64_t)32, m - base);
         for (int j = 0; j < cnt; ++j) e = __dadd_rn(e, __shfl_sync(kFull, t, j));
     }
     return e;
 }
 
 template <bool GIBBS, bool RANDOM_ORDER>
-__device__ __forceinline__ void anneal_read(const ProblemDev &P,
-                                            const int8_t *src, int8_t *dst,
-                                            double *energy_out, double *de,
-                                            int8_t *sp, uint64_t *ring,
+__device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *src,
+                                            int8_t *dst, double *energy_out,
+                                            double *de, int8_t *sp,
+                                            double *scratch, uint64_t *ring,
                                             RingState &rs, unsigned lane,
                                             Counters &cnt) {
-    load_state(P, src, de, sp, lane);
-    if (RANDOM_ORDER)
-        sweep_random<GIBBS>(P, de, sp, ring, rs, lane, cnt);
-    else
-        sweep_sequential<GIBBS>(P, de, sp, ring, rs, lane, cnt);
+    load_state(PD, src, de, sp, lane);
+    {
+        const Prob P = load_prob(PD);
+        if (RANDOM_ORDER)
+            sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
+        else
+            sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
+    }
     __syncwarp();
-    const double e = state_energy(P, sp, lane);
-    for (int v = lane; v < P.n; v += 32) dst[v] = sp[v];
+    const double e = state_energy(PD, sp, lane);
+    const int n = PD->n;
+    for (int v = lane; v < n; v += 32) dst[v] = sp[v];
     if (lane == 0) *energy_out = e;
     __syncwarp();
-}
-
-template <bool SMEM>
-__device__ __forceinline__ void anneal_dispatch(const ProblemDev &P,
-                                                const int8_t *src, int8_t *dst,
-                                                double *energy_out, double *de,
-                                                int8_t *sp, uint64_t *ring,
-                                                RingState &rs, unsigned lane,
-                                                Counters &cnt) {
-    const bool gibbs = P.proposal == 0;
-    if (P.varorder == 0) {
-        if (gibbs)
-            anneal_read<true, false>(P, src, dst, energy_out, de, sp, ring, rs, lane, cnt);
-        else
-            anneal_read<false, false>(P, src, dst, energy_out, de, sp, ring, rs, lane, cnt);
-    } else {
-        if (gibbs)
-            anneal_read<true, true>(P, src, dst, energy_out, de, sp, ring, rs, lane, cnt);
-        else
-            anneal_read<false, true>(P, src, dst, energy_out, de, sp, ring, rs, lane, cnt);
-    }
 }
 
 }  // namespace b200sa

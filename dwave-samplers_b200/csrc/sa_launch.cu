@@ -1,6 +1,8 @@
-// Kernel entry point: warps take (problem, read) work items, either from a
-// device work-queue head (persistent mode: one launch for a whole batch) or
-// by a static stride (plain mode: one launch per problem).
+// Kernel entry points: warps take (problem, read) work items, either from a
+// device work-queue head (persistent mode: one launch per bucket) or by a
+// static stride (plain mode: one launch per problem).  One instantiation per
+// acceptance rule, update order and state location, so each keeps only its
+// own path's registers.
 #include <cuda_runtime.h>
 
 #include "sa_kernel.cuh"
@@ -8,6 +10,7 @@
 
 namespace b200sa {
 
+template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
 __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
     sa_warp_kernel(LaunchArgs A, int warps_per_cta, int region_bytes) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -15,11 +18,19 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
     const int wid = (int)(threadIdx.x >> 5);
     uint8_t *region = smem + (size_t)wid * (size_t)region_bytes;
     uint64_t *ring = reinterpret_cast<uint64_t *>(region);
-    double *de_s = reinterpret_cast<double *>(region + kRing * sizeof(uint64_t));
-    int8_t *sp_s = reinterpret_cast<int8_t *>(region + kRing * sizeof(uint64_t) +
-                                              (size_t)A.smem_cap_n * sizeof(double));
+    double *scratch = reinterpret_cast<double *>(region + kRing * sizeof(uint64_t));
     const int64_t gw = (int64_t)blockIdx.x * warps_per_cta + wid;
     const int64_t total_warps = (int64_t)gridDim.x * warps_per_cta;
+    double *de;
+    int8_t *sp;
+    if (SMEM) {
+        de = reinterpret_cast<double *>(region + kRing * sizeof(uint64_t) + kScratchBytes);
+        sp = reinterpret_cast<int8_t *>(region + kRing * sizeof(uint64_t) + kScratchBytes +
+                                        (size_t)A.smem_cap_n * sizeof(double));
+    } else {
+        de = A.scratch_de + gw * A.scratch_stride;
+        sp = A.scratch_s + gw * A.scratch_stride;
+    }
     if (A.shared_stream && gw != 0) return;
 
     RingState rs;
@@ -45,24 +56,16 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
         const int64_t item = A.items[it];
         const int pi = (int)(item >> 32);
         const int r = (int)(item & 0xffffffffll);
-        const ProblemDev &P = A.problems[pi];
-        const int64_t rd = P.read_offset + r;
+        const ProblemDev *PD = &A.problems[pi];
+        const int64_t rd = PD->read_offset + r;
         if (!stream_live) {
             ring_init(ring, rs, A.seeds[rd], lane);
             stream_live = A.shared_stream != 0;
         }
-        const int8_t *src = A.states_in + P.state_offset + (int64_t)r * P.n;
-        int8_t *dst = A.states_out + P.state_offset + (int64_t)r * P.n;
+        const int64_t so = PD->state_offset + (int64_t)r * PD->n;
         Counters cnt = {0ull, 0ull, 0u};
-        if (P.n <= A.smem_cap_n) {
-            anneal_dispatch<true>(P, src, dst, &A.energies[rd], de_s, sp_s, ring,
-                                  rs, lane, cnt);
-        } else {
-            double *de_g = A.scratch_de + gw * A.scratch_stride;
-            int8_t *sp_g = A.scratch_s + gw * A.scratch_stride;
-            anneal_dispatch<false>(P, src, dst, &A.energies[rd], de_g, sp_g, ring,
-                                   rs, lane, cnt);
-        }
+        anneal_read<GIBBS, RANDOM_ORDER>(PD, A.states_in + so, A.states_out + so,
+                                         &A.energies[rd], de, sp, scratch, ring, rs, lane, cnt);
         if (lane == 0) {
             A.stats[rd].flips = cnt.flips;
             A.stats[rd].passes = cnt.passes;
@@ -83,29 +86,102 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
     }
 }
 
-cudaError_t upload_jump_columns(const uint32_t cols[128][4], cudaStream_t stream) {
-    return cudaMemcpyToSymbolAsync(c_jump, cols, sizeof(uint4) * 128, 0,
-                                   cudaMemcpyHostToDevice, stream);
+using KernelFn = void (*)(LaunchArgs, int, int);
+
+static KernelFn kernel_for(int variant) {
+    switch (variant & 7) {
+        case 0: return sa_warp_kernel<false, false, false>;
+        case 1: return sa_warp_kernel<true, false, false>;
+        case 2: return sa_warp_kernel<false, true, false>;
+        case 3: return sa_warp_kernel<true, true, false>;
+        case 4: return sa_warp_kernel<false, false, true>;
+        case 5: return sa_warp_kernel<true, false, true>;
+        case 6: return sa_warp_kernel<false, true, true>;
+        default: return sa_warp_kernel<true, true, true>;
+    }
 }
 
-cudaError_t launch_sa(const LaunchArgs &args, int grid, int warps_per_cta,
-                      int region_bytes, cudaStream_t stream) {
-    const size_t smem = (size_t)warps_per_cta * (size_t)region_bytes;
-    cudaError_t e = cudaFuncSetAttribute(
-        sa_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    sa_warp_kernel<<<grid, warps_per_cta * 32, smem, stream>>>(args, warps_per_cta,
-                                                               region_bytes);
+// Diagnostic: compares the single-precision acceptance bounds with the exact
+// double-precision decisions on pseudo-random arguments, half of them placed
+// within 2^-8 (relative) of the decision boundary.  counts[0..5] =
+// Metropolis {samples, decided fast, fast disagreeing with exact},
+// Gibbs {samples, decided fast, fast disagreeing with exact}.
+__global__ void acceptance_check_kernel(int64_t samples, uint64_t seed,
+                                        unsigned long long *counts) {
+    uint64_t s0 = seed ^ (0x9e3779b97f4a7c15ull * (blockIdx.x * blockDim.x + threadIdx.x + 1));
+    uint64_t s1 = 0x2545f4914f6cdd1dull;
+    for (int i = 0; i < 20; ++i) xs_next(s0, s1);
+    unsigned long long mf = 0, mx = 0, gf = 0, gx = 0, nm = 0, ng = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < samples;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t a = xs_next(s0, s1), b = xs_next(s0, s1), c = xs_next(s0, s1);
+        const double u = (double)(a >> 11) * 0x1p-53;           // [0, 1)
+        const double eps = ((double)(c >> 11) * 0x1p-53 - 0.5) * 0x1p-7;
+        {  // Metropolis: x in (-44.4, 0]
+            const double x = -44.4 * u;
+            uint64_t r = b;
+            if (i & 1) {
+                const double t = exp(x) * kTwo64 * (1.0 + eps);
+                r = t >= kTwo64 ? ~0ull : (uint64_t)t;
+            }
+            const bool exact = exp(x) * kTwo64 > __ull2double_rn(r);
+            const int f = metropolis_fast(x, r);
+            ++nm;
+            if (f >= 0) {
+                ++mf;
+                if ((f != 0) != exact) ++mx;
+            }
+        }
+        {  // Gibbs: z in (-60, 44.4)
+            const double z = -60.0 + 104.4 * u;
+            uint64_t r = b;
+            if (i & 1) {
+                const double t = kTwo64 / (1.0 + exp(z)) * (1.0 + eps);
+                r = t >= kTwo64 ? ~0ull : (uint64_t)t;
+            }
+            const bool exact = kTwo64 > __ull2double_rn(r) * (1.0 + exp(z));
+            const int f = gibbs_fast(z, r);
+            ++ng;
+            if (f >= 0) {
+                ++gf;
+                if ((f != 0) != exact) ++gx;
+            }
+        }
+    }
+    atomicAdd(&counts[0], nm);
+    atomicAdd(&counts[1], mf);
+    atomicAdd(&counts[2], mx);
+    atomicAdd(&counts[3], ng);
+    atomicAdd(&counts[4], gf);
+    atomicAdd(&counts[5], gx);
+}
+
+cudaError_t acceptance_check(int64_t samples, uint64_t seed, unsigned long long *d_counts) {
+    acceptance_check_kernel<<<148 * 4, 256>>>(samples, seed, d_counts);
     return cudaGetLastError();
 }
 
-cudaError_t kernel_occupancy(int warps_per_cta, int region_bytes, int *ctas_per_sm) {
+cudaError_t upload_jump_table(const uint32_t table[][4], cudaStream_t stream) {
+    return cudaMemcpyToSymbolAsync(g_jump_nib, table, sizeof(uint4) * kJumpTable, 0,
+                                   cudaMemcpyHostToDevice, stream);
+}
+
+cudaError_t launch_sa(int variant, const LaunchArgs &args, int grid, int warps_per_cta,
+                      int region_bytes, cudaStream_t stream) {
+    const KernelFn k = kernel_for(variant);
     const size_t smem = (size_t)warps_per_cta * (size_t)region_bytes;
-    cudaError_t e = cudaFuncSetAttribute(
-        sa_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, sa_warp_kernel,
-                                                         warps_per_cta * 32, smem);
+    k<<<grid, warps_per_cta * 32, smem, stream>>>(args, warps_per_cta, region_bytes);
+    return cudaGetLastError();
+}
+
+cudaError_t kernel_occupancy(int variant, int warps_per_cta, int region_bytes, int *ctas_per_sm) {
+    const KernelFn k = kernel_for(variant);
+    const size_t smem = (size_t)warps_per_cta * (size_t)region_bytes;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k, warps_per_cta * 32, smem);
 }
 
 }  // namespace b200sa

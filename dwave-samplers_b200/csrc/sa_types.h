@@ -2,6 +2,8 @@
 #pragma once
 #include <cstdint>
 
+#include <vector_types.h>
+
 namespace b200sa {
 
 // RNG output ring per read (shared memory).  The ring holds the next
@@ -9,20 +11,20 @@ namespace b200sa {
 // a time, each lane producing kPerLane consecutive outputs from its own
 // segment-start state, and each lane then jumps that state kHalf steps ahead
 // with a precomputed GF(2) matrix (xorshift128+ is linear over GF(2)).
-constexpr int kRing = 512;
+constexpr int kRing = 256;
 constexpr int kHalf = kRing / 2;
 constexpr int kPerLane = kHalf / 32;
 
-// vinfo byte per variable:
-//   bits 0-5: distance to the nearest later neighbour (u - v for the smallest
-//             neighbour u > v), capped at 32.  A flip of v can only change the
-//             decision of a variable inside the current 32-wide window if
-//             that variable is at least this far ahead.
-//   bit 6   : v's adjacency list names some target more than once (self-loop
-//             or repeated coupler), so its updates must run one at a time to
-//             keep the reference's order of additions to the same slot.
-constexpr uint8_t kDistMask = 0x3f;
-constexpr uint8_t kDupFlag = 0x40;
+// Per-variable record (uint2), one load per variable and pass:
+//   x          : start of the variable's adjacency list
+//   y bits 0-23: degree (list length)
+//   y bits 24-31: distance to the nearest later neighbour (u - v for the
+//                smallest neighbour u > v), capped at 32.  A flip of v can
+//                only change the decision of a variable inside the current
+//                32-wide window if that variable is at least this far ahead.
+constexpr uint32_t kDegMask = 0x00ffffffu;
+constexpr int kDistShift = 24;
+constexpr uint32_t kMaxDegree = kDegMask;
 
 struct ProblemDev {
     int32_t n;
@@ -32,11 +34,15 @@ struct ProblemDev {
     int64_t m;              // couplers
     int64_t state_offset;   // element offset of read 0 in the state arrays
     int64_t read_offset;    // offset of read 0 in energies / seeds / stats
-    const int32_t *row;     // [n+1] adjacency offsets
+    const uint2 *vinfo;     // [n] per-variable record (see above)
+    const uint8_t *dist;    // [n] the record's distance field alone (compact, L1-resident)
+    // [n] conflict mask: bit 0 set when v's list names a target twice; bit j
+    // (1..31) set when v and v + j have a common neighbour.  Two committed
+    // flips can add into the same slot only through one of these.
+    const uint32_t *share;
     const int32_t *col;     // [2m] neighbour index, coupler input order
     const double *w;        // [2m] coupling
     const double *h;        // [n]
-    const uint8_t *vinfo;   // [n]
     const int32_t *cu;      // [m] COO, input order (energy)
     const int32_t *cv;      // [m]
     const double *cw;       // [m]
@@ -44,6 +50,10 @@ struct ProblemDev {
     const double *thresholds;  // [num_betas] 44.36142 / beta, host-divided
     int32_t varorder;       // 0 sequential, 1 random
     int32_t proposal;       // 0 Gibbs, 1 Metropolis
+    // Every adjacency list has this length (1..32) and list v starts at
+    // v * regular_degree; 0 when the lists differ in length.
+    int32_t regular_degree;
+    uint32_t regular_magic;  // ceil(2^16 / regular_degree): t / D == (t * magic) >> 16 for t < 1024
 };
 
 // Per-read counters written by the kernel.
@@ -74,8 +84,21 @@ struct LaunchArgs {
     int64_t num_slots;
 };
 
+// Nibble tables of the RNG jump matrix: entry [k][v] is the jump applied to
+// the state whose only set bits are the nibble value v at nibble position k.
+constexpr int kJumpNibbles = 32;
+constexpr int kJumpTable = kJumpNibbles * 16;
+
 // Shared-stream carry layout (uint64 words).
 constexpr int kCarryLaneWords = 64;                 // 32 lanes x 2 words
 constexpr int kCarryWords = kRing + kCarryLaneWords + 2;  // ring, lanes, q, base
+
+// Per-warp shared region: RNG ring, conflict scratch (32 doubles + 32 lane
+// indices), delta energies, spins.
+constexpr int kScratchBytes = 32 * 8 + 32 * 4;
+inline int region_bytes_for(int cap_n) {
+    const int spins = (cap_n + 15) & ~15;
+    return kRing * 8 + kScratchBytes + cap_n * 8 + spins;
+}
 
 }  // namespace b200sa

@@ -134,7 +134,8 @@ B200SA_API int b200sa_plan_layout(b200sa_plan plan, int64_t *state_offsets,
 
 /* Anneal on the device.  d_states_in may equal d_states_out.  d_seeds may be
  * NULL (the seeds given at plan creation are used).  `stream` is a
- * cudaStream_t (NULL = the plan's own stream).  The call returns after the
+ * cudaStream_t; NULL selects the plan's own stream (pass cudaStreamLegacy for
+ * the legacy default stream).  The call returns after the
  * work is enqueued when `sync` is 0, and after it completes when 1 (stats
  * are filled only when sync is 1). */
 B200SA_API int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
@@ -143,6 +144,14 @@ B200SA_API int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_s
                     b200sa_stats *stats, char *err, size_t errlen);
 
 B200SA_API int b200sa_plan_destroy(b200sa_plan plan);
+
+/* Diagnostic, no reference counterpart: checks on the device that the
+ * single-precision acceptance bounds used before the exact double-precision
+ * test never disagree with it.  counts[6] = Metropolis {samples, decided by
+ * the bounds, disagreements}, Gibbs {samples, decided by the bounds,
+ * disagreements}; both disagreement counts must be 0. */
+B200SA_API int b200sa_check_acceptance(int64_t samples, uint64_t seed, int32_t device,
+                                       int64_t counts[6], char *err, size_t errlen);
 
 /* Version string of this library. */
 B200SA_API const char *b200sa_version(void);

@@ -319,3 +319,44 @@ def test_plan_device_buffers_repeatable():
         ws, we = oracle.run(p0.h, p0.u, p0.v, p0.J, p0.states, 1, p0.betas, p0.seeds)
         got = out1[: p0.num_reads * p0.n].cpu().numpy().reshape(p0.num_reads, p0.n)
         np.testing.assert_array_equal(got, ws)
+
+
+def test_plan_runs_on_the_callers_stream():
+    """Work enqueued without sync lands on the given stream (events on that
+    stream bracket it), including torch's default stream."""
+    import torch
+    probs = workloads.uneven_batch(num_problems=3, n_range=(500, 900), reads_range=(64, 96),
+                                   sweeps_range=(200, 300), seed=29)
+    with Plan(probs) as plan:
+        host = np.concatenate([p.states.ravel() for p in probs])
+        sin = torch.from_numpy(host).cuda()
+        out = torch.empty_like(sin)
+        en = torch.empty(plan.total_reads, dtype=torch.float64, device="cuda")
+        ref = plan.run(sin, out, en, sync=True)["kernel_ms"]
+        for stream in (torch.cuda.Stream(), torch.cuda.default_stream()):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plan.run(sin, out, en, stream=stream, sync=False)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            assert e0.elapsed_time(e1) > 0.5 * ref
+
+
+def test_fast_acceptance_bounds_never_disagree_with_exact():
+    """The single-precision log2-domain bounds decide most draws; wherever they
+    decide, the decision must equal the exact double-precision one."""
+    from b200sa import _lib
+    L = _lib.load()
+    counts = np.zeros(6, dtype=np.int64)
+    err = _lib.errbuf()
+    for seed in (1, 2):
+        rc = L.b200sa_check_acceptance(1 << 24, seed, 0, counts.ctypes.data, err, len(err))
+        _lib.check(rc, err)
+        nm, mf, mx, ng, gf, gx = map(int, counts)
+        assert nm == ng == 1 << 24
+        assert mx == 0 and gx == 0
+        # Half the samples sit within 2^-8 (relative) of the boundary on
+        # purpose; the 2^-10 band holds about a fifth of those (and, for
+        # Gibbs with z < -24, every sample clamped onto rand = 2^64 - 1).
+        assert mf > 0.75 * nm and gf > 0.75 * ng

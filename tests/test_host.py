@@ -192,16 +192,36 @@ def _model_anneal(h, u, v, J, s, betas, spb, seed, gibbs):
                             acc[k] = math.exp(-d * beta) * 2.0 ** 64 > r
                 commit = min([L] + [k + dist[p + k] for k in range(L) if acc[k]])
                 R.q += sum(need[:commit])
-                for k in range(commit):
-                    if acc[k]:
-                        var = p + k
-                        m = float(np.int8(4 * s[var]))
-                        for t, w in rows[var]:
-                            de[t] += m * w * s[t]
-                        s[var] = -s[var]
-                        de[var] = -de[var]
+                flips = [p + k for k in range(commit) if acc[k]]
+                if flips:
+                    _model_apply_flips(rows, de, s, flips)
                 p += commit
     return np.array(s, np.int8)
+
+
+def _model_apply_flips(rows, de, s, flips):
+    """The kernel's update rounds: the flips' adjacency entries concatenated
+    in variable order, 32 per round; entries of a round naming the same slot
+    are summed in entry order by the first of them."""
+    entries = []
+    for var in flips:
+        m = float(np.int8(4 * s[var]))
+        entries += [(t, (m * w) * s[t]) for t, w in rows[var]]
+    for base in range(0, len(entries), 32):
+        rnd = entries[base:base + 32]
+        done = set()
+        for i, (t, x) in enumerate(rnd):
+            if t in done:
+                continue
+            acc = de[t]
+            for t2, x2 in rnd[i:]:
+                if t2 == t:
+                    acc = acc + x2
+            de[t] = acc
+            done.add(t)
+    for var in flips:
+        s[var] = -s[var]
+        de[var] = -de[var]
 
 
 @pytest.mark.parametrize("gibbs", [False, True])
