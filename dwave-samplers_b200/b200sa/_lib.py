@@ -36,6 +36,7 @@ EXPORTS = (
     "b200sa_plan_destroy",
     "b200sa_version",
     "b200sa_check_acceptance",
+    "b200sa_sample_noalloc",
 )
 
 
@@ -113,6 +114,11 @@ def load() -> ctypes.CDLL:
     L.b200sa_check_acceptance.restype = c.c_int
     L.b200sa_check_acceptance.argtypes = [c.c_int64, c.c_uint64, c.c_int32, c.c_void_p,
                                           c.c_char_p, c.c_size_t]
+    L.b200sa_sample_noalloc.restype = c.c_int
+    L.b200sa_sample_noalloc.argtypes = [
+        c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32,
+        c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32, c.c_int32, c.c_void_p, c.c_void_p,
+        c.c_int32, c.c_int32, c.c_int32, c.c_void_p, c.c_char_p, c.c_size_t]
     L.b200sa_version.restype = c.c_char_p
     L.b200sa_version.argtypes = []
     _lib = L

@@ -145,6 +145,31 @@ B200SA_API int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_s
 
 B200SA_API int b200sa_plan_destroy(b200sa_plan plan);
 
+/* No counterpart in the reference.  The sampler for callers that cannot
+ * allocate device memory while they run (all device memory owned by a
+ * pre-sized pool or arena, plugin hosts that allow allocation only at
+ * start-up, loops where cudaMalloc/cudaFree and their implicit device-wide
+ * synchronization are not acceptable).  Every pointer is DEVICE memory owned
+ * by the caller: inputs h, couplers, beta schedule, per-read seeds and initial
+ * states; outputs final states and energies.  The call allocates nothing: its
+ * working memory is one fixed 4 MiB array inside the library, held on each
+ * device that loads the library until the process exits, which limits the
+ * problem to num_vars <= 4096, num_couplers <= 65536, num_betas <= 16384 and
+ * num_reads <= 16384 (larger problems return B200SA_EINVAL).  Per-read seeds
+ * only (read r equals a reference call with num_samples=1, seed=seeds[r]).
+ * All calls on a device share that array: calls that overlap on the GPU race
+ * and must be serialized by the caller.  The first call on a device sets the
+ * array up (device address, RNG tables); make it before any stream capture.
+ * `stream` is a cudaStream_t (NULL = legacy default stream); the call returns
+ * when the work is complete.  Returns num_reads or a negative error. */
+B200SA_API int b200sa_sample_noalloc(
+    int32_t num_vars, const double *d_h, int64_t num_couplers, const int32_t *d_coupler_starts,
+    const int32_t *d_coupler_ends, const double *d_coupler_weights, int32_t num_reads,
+    const int8_t *d_states_in, int8_t *d_states_out, double *d_energies,
+    int32_t sweeps_per_beta, int32_t num_betas, const double *d_beta_schedule,
+    const uint64_t *d_seeds, int32_t varorder, int32_t proposal, int32_t device, void *stream,
+    char *err, size_t errlen);
+
 /* Diagnostic, no reference counterpart: checks on the device that the
  * single-precision acceptance bounds used before the exact double-precision
  * test never disagree with it.  counts[6] = Metropolis {samples, decided by
