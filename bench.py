@@ -58,6 +58,17 @@ def parse_args():
     return ap.parse_args()
 
 
+def max_over_ranks(x: float, world: int, device=None) -> float:
+    """Max of a per-rank scalar over all ranks (timings: the slowest rank)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload(args, rank=0):
     probs = workloads.uneven_batch(num_problems=args.problems)
     if args.sweep_scale != 1.0:
@@ -319,13 +330,6 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     probs = workload(args, rank)
     attempts = int(sum(p.attempts for p in probs))
     plan = Plan(probs, device=local)
@@ -353,7 +357,7 @@ def run_ours(args):
 
     with Clocks(local) as clk:
         total_ms = timed("persistent", args.warmup, args.steps)
-    total_ms = max_over_ranks(total_ms)
+    total_ms = max_over_ranks(total_ms, world, "cuda")
     ms_step = total_ms / args.steps
     value = world * attempts / (ms_step / 1000.0)
 
@@ -377,13 +381,13 @@ def run_ours(args):
                         "peak_source": peak_src,
                         "algorithmic_bytes_per_launch": abytes}
     line["clocks"] = clk.summary()
-    line["gpu_launches"] = args.steps
+    line["gpu_launches"] = args.steps * int(stats["launches"])
     line["counters"] = {"flips": flips, "near_ties": stats["near_ties"],
                         "attempts_per_pass": attempts / max(stats["passes"], 1),
                         "check_run_kernel_ms": stats["kernel_ms"]}
 
     if not args.no_plain:
-        plain_ms = max_over_ranks(timed("plain", 1, args.plain_steps)) / args.plain_steps
+        plain_ms = max_over_ranks(timed("plain", 1, args.plain_steps), world, "cuda") / args.plain_steps
         line["plain"] = {"value": world * attempts / (plain_ms / 1000.0), "ms_per_step": plain_ms,
                          "launches_per_step": len(probs)}
         line["batched_over_plain"] = plain_ms / ms_step
@@ -400,7 +404,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         sample_batch(work, mode="persistent", device=local)
         dt = time.perf_counter() - t0
-        e2e_times.append(max_over_ranks(dt))
+        e2e_times.append(max_over_ranks(dt, world, "cuda"))
     if e2e_times:
         e2e = statistics.median(e2e_times[1:])
         line["e2e"] = {"value": world * attempts / e2e, "unit": UNIT, "h2d_bytes_per_step": bi,

@@ -37,6 +37,7 @@ EXPORTS = (
     "b200sa_version",
     "b200sa_check_acceptance",
     "b200sa_sample_noalloc",
+    "b200sa_edge_moments",
 )
 
 
@@ -48,6 +49,7 @@ class Stats(ctypes.Structure):
         ("near_ties", ctypes.c_int64),
         ("passes", ctypes.c_int64),
         ("kernel_ms", ctypes.c_double),
+        ("launches", ctypes.c_int64),
     ]
 
     def as_dict(self) -> dict:
@@ -71,6 +73,19 @@ class Problem(ctypes.Structure):
         ("seeds", ctypes.c_void_p),
         ("varorder", ctypes.c_int32),
         ("proposal", ctypes.c_int32),
+    ]
+
+
+class MomentsProblem(ctypes.Structure):
+    _fields_ = [
+        ("num_vars", ctypes.c_int32),
+        ("num_couplers", ctypes.c_int64),
+        ("num_reads", ctypes.c_int32),
+        ("states", ctypes.c_void_p),
+        ("coupler_starts", ctypes.c_void_p),
+        ("coupler_ends", ctypes.c_void_p),
+        ("sum_s", ctypes.c_void_p),
+        ("sum_ss", ctypes.c_void_p),
     ]
 
 
@@ -119,6 +134,9 @@ def load() -> ctypes.CDLL:
         c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32,
         c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32, c.c_int32, c.c_void_p, c.c_void_p,
         c.c_int32, c.c_int32, c.c_int32, c.c_void_p, c.c_char_p, c.c_size_t]
+    L.b200sa_edge_moments.restype = c.c_int
+    L.b200sa_edge_moments.argtypes = [c.POINTER(MomentsProblem), c.c_int32, c.c_int32,
+                                      c.c_void_p, c.c_char_p, c.c_size_t]
     L.b200sa_version.restype = c.c_char_p
     L.b200sa_version.argtypes = []
     _lib = L

@@ -1,0 +1,221 @@
+"""Differentiable fixed-beta sampling (no reference counterpart).
+
+For Ising models in the reference's convention (energy
+``E(s) = sum_i h_i s_i + sum_c J_c s_u s_v``, ``cpu_sa.cpp:210-227``, and
+acceptance ``exp(-beta dE)``, ``cpu_sa.cpp:154``) the log partition function
+``log Z = log sum_s exp(-beta E(s))`` has
+
+    d log Z / d h_i = -beta <s_i>,     d log Z / d J_c = -beta <s_u(c) s_v(c)>.
+
+:class:`LogPartition` wraps fixed-beta sampling on the B200 (every read bit
+identical to the reference run with that read's seed) as an autograd
+``Function``: its forward draws the samples, its backward reduces them over
+the couplers with the ``b200sa_edge_moments`` CUDA kernel and returns the two
+expectations above scaled by ``-beta``.  The forward *value* is a placeholder
+(zero): only the gradient of log Z is estimated.
+
+When ``reads * num_vars`` exceeds ``memory_budget`` bytes the samples are not
+kept: the backward re-runs the sampler from the stored seeds in chunks of
+reads.  Initial states are then a deterministic function of ``init_seed`` (not
+stored either), so the recomputed samples are bit-identical.
+
+``models`` may hold many problems; sampling runs as one persistent batch and
+the backward reduction as one launch over all of them.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .batch import Plan
+from .workloads import Instance
+
+
+@dataclass
+class IsingModel:
+    """Structure of one model: size and couplers (COO, input order)."""
+    num_vars: int
+    u: np.ndarray  # int32 [m]
+    v: np.ndarray  # int32 [m]
+
+    @property
+    def num_couplers(self) -> int:
+        return int(self.u.shape[0])
+
+
+def _mix64(x: np.ndarray) -> np.ndarray:
+    """splitmix64 finalizer (a bijective 64-bit mixing function), vectorized."""
+    with np.errstate(over="ignore"):
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        return x ^ (x >> np.uint64(31))
+
+
+def initial_states(init_seed: int, model_index: int, reads: int, n: int,
+                   read0: int = 0) -> np.ndarray:
+    """Uniform +-1 initial states as a counter-based hash of (seed, model,
+    read, variable): any range of reads can be regenerated identically."""
+    r = np.arange(read0, read0 + reads, dtype=np.uint64)[:, None]
+    i = np.arange(n, dtype=np.uint64)[None, :]
+    with np.errstate(over="ignore"):
+        key = _mix64(np.uint64(init_seed) * np.uint64(0x9E3779B97F4A7C15)
+                     + np.uint64(model_index) * np.uint64(0xD1B54A32D192ED03))
+        x = _mix64(key ^ (r * np.uint64(0x100000001B3) + i))
+    return np.where((x >> np.uint64(63)) != 0, 1, -1).astype(np.int8)
+
+
+def read_seeds(seed: int, model_index: int, reads: int, read0: int = 0) -> np.ndarray:
+    base = (np.uint64(seed) * np.uint64(1000003) + np.uint64(model_index) * np.uint64(1 << 40))
+    with np.errstate(over="ignore"):
+        return base + np.arange(read0, read0 + reads, dtype=np.uint64)
+
+
+def sample_models(models: Sequence[IsingModel], hs: Sequence[np.ndarray],
+                  Js: Sequence[np.ndarray], beta: float, sweeps: int, reads: int,
+                  seed: int, init_seed: int, read0: int = 0, proposal: str = "Gibbs",
+                  device: int = 0) -> list[torch.Tensor]:
+    """Fixed-beta sampling of every model (one persistent batch): reads
+    [read0, read0 + reads) of each model, `sweeps` sweeps at `beta`.
+    Returns one int8 CUDA tensor (reads x n) per model."""
+    insts = []
+    for k, (mod, h, J) in enumerate(zip(models, hs, Js)):
+        insts.append(Instance(
+            np.ascontiguousarray(h, dtype=np.float64), mod.u, mod.v,
+            np.ascontiguousarray(J, dtype=np.float64),
+            initial_states(init_seed, k, reads, mod.num_vars, read0),
+            np.array([float(beta)]), int(sweeps), read_seeds(seed, k, reads, read0),
+            proposal=proposal))
+    dev = torch.device("cuda", device)
+    with Plan(insts, device=device) as plan:
+        host = np.concatenate([p.states.ravel() for p in insts])
+        sin = torch.from_numpy(host).to(dev)
+        sout = torch.empty_like(sin)
+        en = torch.empty(plan.total_reads, dtype=torch.float64, device=dev)
+        plan.run(sin, sout, en, stream=torch.cuda.current_stream(dev), sync=True)
+        offs = plan.state_offsets
+    return [sout[int(offs[k]):int(offs[k + 1])].view(reads, insts[k].n) for k in range(len(insts))]
+
+
+def edge_moments(models: Sequence[IsingModel], samples: Sequence[torch.Tensor],
+                 device: int = 0):
+    """Integer sums over reads of s_i and of s_u s_v per coupler, for every
+    model, in one launch of the moments kernel.  Returns lists of int64 CUDA
+    tensors (n,) and (m,)."""
+    dev = torch.device("cuda", device)
+    keep = []
+    arr = (_lib.MomentsProblem * max(len(models), 1))()
+    sums_s, sums_ss = [], []
+    for k, (mod, st) in enumerate(zip(models, samples)):
+        st = st.contiguous()
+        cu = torch.from_numpy(np.ascontiguousarray(mod.u, dtype=np.int32)).to(dev)
+        cv = torch.from_numpy(np.ascontiguousarray(mod.v, dtype=np.int32)).to(dev)
+        ss = torch.zeros(mod.num_vars, dtype=torch.int64, device=dev)
+        sss = torch.zeros(max(mod.num_couplers, 1), dtype=torch.int64, device=dev)
+        keep += [st, cu, cv]
+        q = arr[k]
+        q.num_vars = mod.num_vars
+        q.num_couplers = mod.num_couplers
+        q.num_reads = int(st.shape[0])
+        q.states = st.data_ptr()
+        q.coupler_starts = cu.data_ptr()
+        q.coupler_ends = cv.data_ptr()
+        q.sum_s = ss.data_ptr()
+        q.sum_ss = sss.data_ptr()
+        sums_s.append(ss)
+        sums_ss.append(sss[:mod.num_couplers])
+    err = _lib.errbuf()
+    rc = _lib.load().b200sa_edge_moments(arr, len(models), device,
+                                         torch.cuda.current_stream(dev).cuda_stream, err, len(err))
+    _lib.check(rc, err)
+    del keep
+    return sums_s, sums_ss
+
+
+class LogPartition(torch.autograd.Function):
+    """``LogPartition.apply(h_cat, J_cat, spec)`` for a batch of models.
+
+    ``h_cat`` / ``J_cat`` are the models' fields and couplings concatenated
+    (float64, any device, may require grad); ``spec`` is a
+    :class:`SamplingSpec`.  Returns a zero placeholder (log Z itself is not
+    estimated); the forward's samples are left in ``spec.last_samples``
+    (empty when they are recomputed in backward).  Backward returns
+    ``-beta <s_i>`` and ``-beta <s_u s_v>`` per coupler.
+    """
+
+    @staticmethod
+    def forward(ctx, h_cat, J_cat, spec):
+        hs, Js = spec.split(h_cat.detach().cpu().numpy(), J_cat.detach().cpu().numpy())
+        keep = spec.reads * sum(m.num_vars for m in spec.models) <= spec.memory_budget
+        samples = []
+        if keep:
+            samples = sample_models(spec.models, hs, Js, spec.beta, spec.sweeps, spec.reads,
+                                    spec.seed, spec.init_seed, 0, spec.proposal, spec.device)
+        spec.last_samples = samples
+        ctx.spec = spec
+        ctx.hs, ctx.Js = hs, Js
+        ctx.samples = samples
+        ctx.h_device, ctx.J_device = h_cat.device, J_cat.device
+        return torch.zeros((), dtype=torch.float64, device=h_cat.device)
+
+    @staticmethod
+    def backward(ctx, g):
+        spec = ctx.spec
+        sum_s, sum_ss = spec.moments(ctx.hs, ctx.Js, ctx.samples)
+        spec.last_moments = (sum_s, sum_ss)
+        scale = -spec.beta / spec.reads
+        gh = (torch.cat([x.to(torch.float64) for x in sum_s]) * scale).to(ctx.h_device)
+        gJ = (torch.cat([x.to(torch.float64) for x in sum_ss]) * scale).to(ctx.J_device)
+        return gh * g.to(ctx.h_device), gJ * g.to(ctx.J_device), None
+
+
+@dataclass
+class SamplingSpec:
+    """Fixed-beta sampling settings for :class:`LogPartition`."""
+    models: Sequence[IsingModel]
+    beta: float = 1.0
+    sweeps: int = 1000
+    reads: int = 1024
+    seed: int = 1
+    init_seed: int = 2
+    proposal: str = "Gibbs"
+    memory_budget: int = 1 << 30   # bytes of samples kept for backward
+    recompute_chunk: int = 256     # reads per chunk when recomputing
+    device: int = 0
+    last_samples: list = None      # set by LogPartition.forward
+    last_moments: tuple = None     # set by LogPartition.backward
+
+    def split(self, h_cat, J_cat):
+        hs, Js, i, j = [], [], 0, 0
+        for m in self.models:
+            hs.append(h_cat[i:i + m.num_vars])
+            Js.append(J_cat[j:j + m.num_couplers])
+            i += m.num_vars
+            j += m.num_couplers
+        return hs, Js
+
+    def moments(self, hs, Js, samples):
+        if samples:
+            return edge_moments(self.models, samples, self.device)
+        # Recompute from the stored seeds, chunk by chunk of reads.
+        tot_s = tot_ss = None
+        for r0 in range(0, self.reads, self.recompute_chunk):
+            k = min(self.recompute_chunk, self.reads - r0)
+            chunk = sample_models(self.models, hs, Js, self.beta, self.sweeps, k, self.seed,
+                                  self.init_seed, r0, self.proposal, self.device)
+            s, ss = edge_moments(self.models, chunk, self.device)
+            if tot_s is None:
+                tot_s, tot_ss = s, ss
+            else:
+                tot_s = [a + b for a, b in zip(tot_s, s)]
+                tot_ss = [a + b for a, b in zip(tot_ss, ss)]
+        return tot_s, tot_ss
+
+
+def log_partition(h_cat: torch.Tensor, J_cat: torch.Tensor, spec: SamplingSpec):
+    """Differentiable placeholder for log Z (see :class:`LogPartition`)."""
+    return LogPartition.apply(h_cat, J_cat, spec)

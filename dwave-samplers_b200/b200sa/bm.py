@@ -1,0 +1,90 @@
+"""Batched Boltzmann-machine learning on the B200 sampler (no reference
+counterpart).
+
+Fully visible Ising models in the reference's convention
+(``p(s) ~ exp(-beta E(s))``, ``E = sum h s + sum J s s``).  The negative
+log-likelihood of data with coupler correlations ``<s_u s_v>_data`` is
+
+    NLL(J) = beta * sum_c J_c <s_u s_v>_data + log Z(J)
+
+whose gradient ``beta <ss>_data - beta <ss>_model`` is obtained by autograd:
+the data term is a torch expression and ``log Z`` is
+:class:`b200sa.autograd.LogPartition` (fixed-beta Gibbs sampling forward,
+moments kernel backward).  All models are sampled in one persistent batch and
+reduced in one moments launch per step; Adam updates the couplings.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from typing import Callable, Sequence
+
+import numpy as np
+import torch
+
+from .autograd import IsingModel, SamplingSpec, edge_moments, log_partition, sample_models
+
+
+@dataclass
+class BMResult:
+    J: list                      # fitted couplings per model (numpy)
+    corr_error: list = field(default_factory=list)  # mean |<ss>_model - <ss>_data| per step
+    step_seconds: list = field(default_factory=list)
+    target_seconds: float = 0.0
+
+    @property
+    def steps_per_second(self) -> float:
+        t = sum(self.step_seconds)
+        return len(self.step_seconds) / t if t > 0 else float("nan")
+
+
+def target_correlations(models: Sequence[IsingModel], hs, Js, beta: float, reads: int,
+                        sweeps: int, seed: int, device: int = 0):
+    """<s_u s_v> per coupler of the ground-truth models, from `reads` fixed-beta
+    Gibbs reads of `sweeps` sweeps each."""
+    samples = sample_models(models, hs, Js, beta, sweeps, reads, seed, seed + 1, 0, "Gibbs",
+                            device)
+    _, sss = edge_moments(models, samples, device)
+    return [x.to(torch.float64) / reads for x in sss]
+
+
+def fit(truth: Sequence[tuple], beta: float = 1.0, steps: int = 500, reads: int = 1024,
+        sweeps: int = 2000, lr: float = 1e-2, target_reads: int = 8192,
+        target_sweeps: int = 2000, seed: int = 11, device: int = 0,
+        callback: Callable[[int, float], None] | None = None) -> BMResult:
+    """Fit J (from zero, h fixed at the truth's h) to the truth's coupler
+    correlations.  `truth` is a list of (h, u, v, J) ground-truth models."""
+    dev = torch.device("cuda", device)
+    models = [IsingModel(len(h), np.ascontiguousarray(u, np.int32), np.ascontiguousarray(v, np.int32))
+              for h, u, v, _ in truth]
+    hs = [np.asarray(h, np.float64) for h, _, _, _ in truth]
+    t0 = time.perf_counter()
+    corr_data = target_correlations(models, hs, [np.asarray(J, np.float64) for *_, J in truth],
+                                    beta, target_reads, target_sweeps, seed, device)
+    torch.cuda.synchronize(dev)
+    res = BMResult(J=[], target_seconds=time.perf_counter() - t0)
+    data = torch.cat(corr_data).to(dev)
+    h_cat = torch.from_numpy(np.concatenate(hs)).to(dev)
+    J = torch.zeros(data.shape[0], dtype=torch.float64, device=dev, requires_grad=True)
+    opt = torch.optim.Adam([J], lr=lr)
+    for step in range(steps):
+        t = time.perf_counter()
+        spec = SamplingSpec(models, beta=beta, sweeps=sweeps, reads=reads,
+                            seed=seed + 1000 + step, init_seed=seed + 7 + step, device=device)
+        loss = beta * torch.dot(J, data) + log_partition(h_cat, J, spec)
+        opt.zero_grad()
+        loss.backward()
+        opt.step()
+        model_corr = torch.cat([x.to(torch.float64) for x in spec.last_moments[1]]) / reads
+        err = float(torch.mean(torch.abs(model_corr - data)))
+        torch.cuda.synchronize(dev)
+        res.step_seconds.append(time.perf_counter() - t)
+        res.corr_error.append(err)
+        if callback is not None:
+            callback(step, err)
+    Jn = J.detach().cpu().numpy()
+    off = 0
+    for m in models:
+        res.J.append(Jn[off:off + m.num_couplers].copy())
+        off += m.num_couplers
+    return res

@@ -88,8 +88,8 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
         out.w[k] = J;
     }
     // Speculation info: nearest later neighbour; repeated targets; pairs of
-    // variables less than 32 apart with a common neighbour.
-    out.share.assign((size_t)n, 0u);
+    // variables less than 64 apart with a common neighbour.
+    out.share.assign((size_t)n, 0ull);
     {
         std::vector<int32_t> nb;
         for (int32_t u = 0; u < n; ++u) {
@@ -97,15 +97,15 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
             std::sort(nb.begin(), nb.end());
             nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
             for (size_t i = 0; i < nb.size(); ++i)
-                for (size_t j = i + 1; j < nb.size() && nb[j] - nb[i] < 32; ++j)
-                    out.share[nb[i]] |= 1u << (nb[j] - nb[i]);
+                for (size_t j = i + 1; j < nb.size() && nb[j] - nb[i] < 64; ++j)
+                    out.share[nb[i]] |= 1ull << (nb[j] - nb[i]);
         }
     }
     std::vector<int32_t> mark((size_t)n, -1);
     int32_t maxdeg = 0;
     bool any_dup = false;
     for (int32_t v = 0; v < n; ++v) {
-        uint32_t dist = 32;
+        uint32_t dist = kDistCap;
         const int32_t e0 = out.row[v], e1 = out.row[v + 1];
         maxdeg = std::max(maxdeg, e1 - e0);
         for (int32_t e = e0; e < e1; ++e) {
@@ -113,7 +113,7 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
             if (u > v) dist = std::min<uint32_t>(dist, (uint32_t)(u - v));
             if (mark[u] == v) {
                 any_dup = true;
-                out.share[v] |= 1u;
+                out.share[v] |= 1ull;
             }
             mark[u] = v;
         }

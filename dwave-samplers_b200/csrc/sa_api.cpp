@@ -110,7 +110,7 @@ const uint32_t (*jump_table())[4] {
 // warps per SM; the last size class keeps its state in global memory.
 constexpr int kSizeClasses = 8;
 constexpr int kGlobalClass = kSizeClasses - 1;
-constexpr int kKinds = 4;
+constexpr int kKinds = 8;
 constexpr int kBuckets = kSizeClasses * kKinds;
 constexpr int kStreams = 8;
 const int kClassBound[kSizeClasses - 2] = {128, 256, 512, 1024, 2048, 4096};
@@ -122,7 +122,18 @@ int size_class(int n, int onchip_max) {
     return kSizeClasses - 2;
 }
 
-int kind_of(const ProblemDev &d) { return (d.proposal == 0 ? 1 : 0) | (d.varorder ? 2 : 0); }
+// Kernel kind of a problem: bit 0 Gibbs, bit 1 random order, bit 2 wide
+// (64-variable) windows.  Wide windows need equal-length lists; measured on
+// the random-regular shapes of the benchmark (n 500-4000, degree 6-16) they
+// raise attempts per pass by ~40% but the extra update round costs as much,
+// so they are not selected by default.
+bool wide_windows(const ProblemDev &d, bool allow_wide) {
+    return allow_wide && d.varorder == 0 && d.regular_degree > 0;
+}
+
+int kind_of(const ProblemDev &d, bool allow_wide = false) {
+    return (d.proposal == 0 ? 1 : 0) | (d.varorder ? 2 : 0) | (wide_windows(d, allow_wide) ? 4 : 0);
+}
 
 }  // namespace
 
@@ -155,6 +166,7 @@ struct b200sa_plan_s {
     int32_t bucket_max_n[kBuckets] = {};
     int64_t bucket_lead_cost[kBuckets] = {};
     std::map<std::pair<int, int>, int> occ_cache;  // (variant*2^24 + warps, region) -> CTAs/SM
+    int64_t launches = 0;  // sweep-kernel launches issued by the current run
 
     ~b200sa_plan_s() {
         if (ev0) cudaEventDestroy(ev0);
@@ -200,7 +212,7 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
     const int smem_blk = (int)P->prop.sharedMemPerBlockOptin;
     const int cap = max_n_here <= P->onchip_max ? max_n_here : 0;
     const int region = region_bytes_for(cap);
-    const int variant = kernel_variant(kind & 1, kind & 2, cap > 0);
+    const int variant = kernel_variant(kind & 1, kind & 2, cap > 0, kind & 4);
     int best_w = 1, best_warps = 0;
     for (int w = 1; w <= kMaxThreadsPerCta / 32; ++w) {
         if ((int64_t)w * region > smem_blk) break;
@@ -288,6 +300,7 @@ int launch_items(b200sa_plan_s *P, LaunchArgs a, int kind, const int64_t *items,
     a.num_slots = P->scratch_slots;
     a.queue_head = (persistent && !shared_stream) ? qhead : nullptr;
     B200SA_CUDA(launch_sa(s.variant, a, s.grid, s.warps_per_cta, s.region, st));
+    P->launches++;
     return B200SA_OK;
 }
 
@@ -433,7 +446,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         Off &o = off[i];
         o.vinfo = take(8 * n);
         o.dist = take(n);
-        o.share = take(4 * n);
+        o.share = take(8 * n);
         o.col = take(4 * 2 * m);
         o.w = take(8 * 2 * m);
         o.h = take(8 * n);
@@ -468,7 +481,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
             std::memcpy(&staging[o.vinfo], adj[i].vinfo.data(), 8 * n);
             for (size_t v = 0; v < n; ++v)
                 staging[o.dist + v] = (uint8_t)(adj[i].vinfo[2 * v + 1] >> kDistShift);
-            std::memcpy(&staging[o.share], adj[i].share.data(), 4 * n);
+            std::memcpy(&staging[o.share], adj[i].share.data(), 8 * n);
             std::memcpy(&staging[o.h], q.h, 8 * n);
         }
         if (nb) {
@@ -497,7 +510,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         d.read_offset = P->read_off[i];
         d.vinfo = reinterpret_cast<const uint2 *>(base + o.vinfo);
         d.dist = base + o.dist;
-        d.share = reinterpret_cast<const uint32_t *>(base + o.share);
+        d.share = reinterpret_cast<const unsigned long long *>(base + o.share);
         d.col = reinterpret_cast<const int32_t *>(base + o.col);
         d.w = reinterpret_cast<const double *>(base + o.w);
         d.h = reinterpret_cast<const double *>(base + o.h);
@@ -611,6 +624,7 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
     if (stats) std::memset(stats, 0, sizeof(*stats));
     LaunchArgs a = base_args(plan, d_states_in, d_states_out, d_energies, d_seeds);
+    plan->launches = 0;
     // Problems with no variables: energies are 0 (cpu_sa.cpp:217-226 over nothing).
     for (int i = 0; i < plan->num_problems; ++i) {
         if (plan->n[i] == 0 && plan->reads[i] > 0)
@@ -644,6 +658,7 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
             for (int i = 0; i < plan->num_problems; ++i)
                 if (plan->n[i] == 0) stats->reads += plan->reads[i];
             stats->kernel_ms = ms;
+            stats->launches = plan->launches;
         }
     }
     return B200SA_OK;

@@ -139,7 +139,7 @@ struct Prob {
     const double *__restrict__ betas;
     const double *__restrict__ thresholds;
     const uint8_t *__restrict__ dist;
-    const uint32_t *__restrict__ share;
+    const unsigned long long *__restrict__ share;
     int regular_degree;
     uint32_t regular_magic;
 };
@@ -350,20 +350,21 @@ __device__ __forceinline__ void apply_flips(const Prob &P, double *de, int8_t *s
     __syncwarp();
 }
 
-// Neighbour updates of the committed flips `fm` for equal-length lists (D
-// entries each, list v at v * D).  The entries of the first 64 accepted flips
-// were loaded into (nb0, w0, k0) / (nb1, w1, k1) before the commit was known
-// (the committed flips are a prefix of the accepted ones, in lane order);
-// later entries are loaded here.  Same grouping rule as apply_flips.
+// Neighbour updates of the committed flips for equal-length lists (D entries
+// each, list v at v * D).  `rank_tab[f]` describes the f-th committed flip in
+// variable order: window position + 256 * (spin before the flip), so the
+// position is its low byte and the spin the arithmetic shift by 8.  The entries of the first 64 accepted flips were loaded
+// into (nb0, w0, k0) / (nb1, w1, k1) before the commit point was known (the
+// committed flips are a prefix of the accepted ones); later entries are
+// loaded here.  Equal targets within a round are summed in entry order by
+// their first lane, as in apply_flips.
 __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t *sp,
-                                               double *scratch, const int *owner_of_rank,
-                                               unsigned fm, int p, int v, int s_old,
-                                               int nb0, double w0, int k0, int nb1,
-                                               double w1, int k1, bool may_conflict,
+                                               double *scratch, const int *rank_tab,
+                                               int nflips, int p, int nb0, double w0, int k0,
+                                               int nb1, double w1, int k1, bool may_conflict,
                                                unsigned lane) {
     const int D = P.regular_degree;
-    const double mult = (double)(int)(int8_t)(4 * s_old);
-    const int total = __popc(fm) * D;
+    const int total = nflips * D;
     for (int base = 0; base < total; base += 32) {
         const int t = base + (int)lane;
         const bool a = t < total;
@@ -377,18 +378,19 @@ __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t
             k = 0, nb = 0, wt = 0.0;
             if (a) {
                 const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
-                k = owner_of_rank[r];
-                const int e = (p + k) * D + (t - r * D);
+                k = rank_tab[r];
+                const int e = (p + (k & 0xff)) * D + (t - r * D);
                 nb = __ldg(&P.col[e]);
                 wt = __ldg(&P.w[e]);
             }
         }
-        const double m_k = __shfl_sync(kFull, mult, k);
         double x = 0.0;
-        if (a)
-            x = __dmul_rn(__dmul_rn(m_k, wt), (double)(int)sp[nb]);
-        else
+        if (a) {
+            const double mult = (double)(int)(int8_t)(4 * (k >> 8));  // cpu_sa.cpp:172
+            x = __dmul_rn(__dmul_rn(mult, wt), (double)(int)sp[nb]);
+        } else {
             nb = -1 - (int)lane;  // distinct per inactive lane
+        }
         const unsigned grp = may_conflict ? __match_any_sync(kFull, nb) : (1u << lane);
         const bool alone = grp == (1u << lane);
         if (a && alone) de[nb] = __dadd_rn(de[nb], x);
@@ -408,22 +410,21 @@ __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t
         }
         __syncwarp();
     }
-    if ((fm >> lane) & 1u) {  // cpu_sa.cpp:189-190, after the variable's own updates
-        sp[v] = (int8_t)(-s_old);
-        de[v] = __dmul_rn(de[v], -1.0);
-    }
-    __syncwarp();
 }
 
-template <bool GIBBS>
+// Sequential order (cpu_sa.cpp:132-192) in speculative passes over windows
+// of 32*S consecutive variables, S per lane (slot s of lane l is window
+// position 32*s + l).
+template <bool GIBBS, int S>
 __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                                                  int8_t *sp, double *scratch,
                                                  uint64_t *ring, RingState &rs,
                                                  unsigned lane, Counters &cnt) {
+    constexpr int W = 32 * S;
     const int n = P.n;
     const int D = P.regular_degree;
     const unsigned lt_mask = (1u << lane) - 1u;
-    int *owner_of_rank = reinterpret_cast<int *>(scratch + 32);
+    int *rank_tab = reinterpret_cast<int *>(scratch + 32);
     for (int b = 0; b < P.num_betas; ++b) {
         const double beta = __ldg(&P.betas[b]);
         const double thr = __ldg(&P.thresholds[b]);
@@ -431,84 +432,144 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
             int p = 0;
             while (p < n) {
                 ring_refill(ring, rs, lane);
-                const int L = min(32, n - p);
-                const int v = p + (int)lane;
-                const bool act = (int)lane < L;
-                double d = 0.0;
-                int dist = 32;
-                unsigned shr = 0u;
-                uint2 vi = make_uint2(0u, 0u);
-                if (act) {
-                    d = de[v];
-                    dist = __ldg(&P.dist[v]);
-                    shr = __ldg(&P.share[v]);
-                    if (!D) vi = __ldg(&P.vinfo[v]);
-                }
-                const bool consider = act && !(d >= thr);  // cpu_sa.cpp:140
-                const bool need = GIBBS ? consider : (consider && !(d <= 0.0));
-                const unsigned need_mask = __ballot_sync(kFull, need);
-                bool acc = GIBBS ? false : consider;  // Metropolis: d <= 0 accepts
-                bool near = false;
-                if (need) {
-                    const uint64_t r =
-                        ring[(rs.q + (uint64_t)__popc(need_mask & lt_mask)) & (kRing - 1)];
-                    const int fast = GIBBS ? gibbs_fast(__dmul_rn(d, beta), r)
-                                           : metropolis_fast(__dmul_rn(-d, beta), r);
-                    if (fast >= 0) {
-                        acc = fast != 0;
-                    } else {
-                        const int ex = GIBBS ? gibbs_exact(d, beta, r) : metropolis_exact(d, beta, r);
-                        acc = (ex & 1) != 0;
-                        near = (ex & 2) != 0;
+                const int L = min(W, n - p);
+                double d[S];
+                int dist[S];
+                unsigned long long shr[S];
+                uint2 vi[S];
+                bool act[S];
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    const int pos = 32 * s + (int)lane;
+                    act[s] = pos < L;
+                    d[s] = 0.0;
+                    dist[s] = (int)kDistCap;
+                    shr[s] = 0ull;
+                    vi[s] = make_uint2(0u, 0u);
+                    if (act[s]) {
+                        d[s] = de[p + pos];
+                        dist[s] = __ldg(&P.dist[p + pos]);
+                        shr[s] = __ldg(&P.share[p + pos]);
+                        if (!D) vi[s] = __ldg(&P.vinfo[p + pos]);
                     }
                 }
-                const unsigned am = __ballot_sync(kFull, acc);
+                unsigned nm[S];
+                bool acc[S], near[S];
+                uint64_t rbase = rs.q;
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    const bool consider = act[s] && !(d[s] >= thr);  // cpu_sa.cpp:140
+                    const bool need = GIBBS ? consider : (consider && !(d[s] <= 0.0));
+                    nm[s] = __ballot_sync(kFull, need);
+                    acc[s] = GIBBS ? false : consider;  // Metropolis: d <= 0 accepts
+                    near[s] = false;
+                    if (need) {
+                        const uint64_t r =
+                            ring[(rbase + (uint64_t)__popc(nm[s] & lt_mask)) & (kRing - 1)];
+                        const int fast = GIBBS ? gibbs_fast(__dmul_rn(d[s], beta), r)
+                                               : metropolis_fast(__dmul_rn(-d[s], beta), r);
+                        if (fast >= 0) {
+                            acc[s] = fast != 0;
+                        } else {
+                            const int ex = GIBBS ? gibbs_exact(d[s], beta, r)
+                                                 : metropolis_exact(d[s], beta, r);
+                            acc[s] = (ex & 1) != 0;
+                            near[s] = (ex & 2) != 0;
+                        }
+                    }
+                    rbase += (uint64_t)__popc(nm[s]);
+                }
+                unsigned am[S];
+                unsigned any_acc = 0u;
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    am[s] = __ballot_sync(kFull, acc[s]);
+                    any_acc |= am[s];
+                }
                 // Equal-length lists: start loading the accepted flips'
                 // adjacency before the commit point is known.
                 int nb0 = 0, nb1 = 0, k0 = 0, k1 = 0;
                 double w0 = 0.0, w1 = 0.0;
-                if (D && am) {
-                    if (acc) owner_of_rank[__popc(am & lt_mask)] = (int)lane;
+                if (D && any_acc) {
+                    int abase = 0;
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        if (acc[s]) {
+                            const int pos = 32 * s + (int)lane;
+                            rank_tab[abase + __popc(am[s] & lt_mask)] =
+                                pos + 256 * (int)sp[p + pos];
+                        }
+                        abase += __popc(am[s]);
+                    }
                     __syncwarp();
-                    const int pre = min(__popc(am) * D, 64);
+                    const int pre = min(abase * D, 64);
                     if ((int)lane < pre) {
                         const int r = (int)((lane * P.regular_magic) >> 16);
-                        k0 = owner_of_rank[r];
-                        const int e = (p + k0) * D + ((int)lane - r * D);
+                        k0 = rank_tab[r];
+                        const int e = (p + (k0 & 0xff)) * D + ((int)lane - r * D);
                         nb0 = __ldg(&P.col[e]);
                         w0 = __ldg(&P.w[e]);
                     }
                     if ((int)lane + 32 < pre) {
                         const int t = (int)lane + 32;
                         const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
-                        k1 = owner_of_rank[r];
-                        const int e = (p + k1) * D + (t - r * D);
+                        k1 = rank_tab[r];
+                        const int e = (p + (k1 & 0xff)) * D + (t - r * D);
                         nb1 = __ldg(&P.col[e]);
                         w1 = __ldg(&P.w[e]);
                     }
                 }
-                const int bound = acc ? (int)lane + dist : 32;
+                int bound = W;
+#pragma unroll
+                for (int s = 0; s < S; ++s)
+                    if (acc[s]) bound = min(bound, 32 * s + (int)lane + dist[s]);
                 const int c = min(__reduce_min_sync(kFull, bound), L);
-                const unsigned commit = c >= 32 ? kFull : ((1u << c) - 1u);
-                rs.q += (uint64_t)__popc(need_mask & commit);
-                const unsigned fm = am & commit;
-                cnt.near += __popc(__ballot_sync(kFull, near) & commit);
-                cnt.flips += __popc(fm);
+                unsigned fm[S];
+                int nflips = 0;
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    const int cs = c - 32 * s;
+                    const unsigned cm = cs >= 32 ? kFull : (cs <= 0 ? 0u : ((1u << cs) - 1u));
+                    rs.q += (uint64_t)__popc(nm[s] & cm);
+                    fm[s] = am[s] & cm;
+                    cnt.near += __popc(__ballot_sync(kFull, near[s]) & cm);
+                    nflips += __popc(fm[s]);
+                }
+                cnt.flips += nflips;
                 cnt.passes += 1;
-                if (fm) {
-                    const int s_old = act ? (int)sp[v] : 0;
+                if (nflips) {
                     // A slot can receive two additions only through a repeated
                     // target in one list or a neighbour common to two flips.
-                    const unsigned later = lane < 31 ? fm >> (lane + 1) : 0u;
-                    const bool f = (fm >> lane) & 1u;
-                    const bool may_conflict =
-                        __any_sync(kFull, f && ((shr & 1u) || ((shr >> 1) & later)));
-                    if (D)
-                        update_regular(P, de, sp, scratch, owner_of_rank, fm, p, v, s_old, nb0,
-                                       w0, k0, nb1, w1, k1, may_conflict, lane);
-                    else
-                        apply_flips(P, de, sp, scratch, fm, v, (int)vi.x,
-                                    (int)(vi.y & kDegMask), s_old, may_conflict, lane);
+                    unsigned long long fm64 = fm[0];
+                    if (S > 1) fm64 |= (unsigned long long)fm[S - 1] << 32;
+                    bool risk = false;
+#pragma unroll
+                    for (int s = 0; s < S; ++s) {
+                        const int pos = 32 * s + (int)lane;
+                        if ((fm[s] >> lane) & 1u) {
+                            const unsigned long long later = pos < 63 ? fm64 >> (pos + 1) : 0ull;
+                            risk |= (shr[s] & 1ull) || ((shr[s] >> 1) & later);
+                        }
+                    }
+                    const bool may_conflict = __any_sync(kFull, risk);
+                    if (D) {
+                        update_regular(P, de, sp, scratch, rank_tab, nflips, p, nb0, w0, k0, nb1,
+                                       w1, k1, may_conflict, lane);
+#pragma unroll
+                        for (int s = 0; s < S; ++s) {
+                            if ((fm[s] >> lane) & 1u) {  // cpu_sa.cpp:189-190
+                                const int v = p + 32 * s + (int)lane;
+                                sp[v] = (int8_t)(-(int)sp[v]);
+                                de[v] = __dmul_rn(de[v], -1.0);
+                            }
+                        }
+                        __syncwarp();
+                    } else if constexpr (S == 1) {
+                        const int v = p + (int)lane;
+                        const int s_old = act[0] ? (int)sp[v] : 0;
+                        apply_flips(P, de, sp, scratch, fm[0], v, (int)vi[0].x,
+                                    (int)(vi[0].y & kDegMask), s_old, may_conflict, lane);
+                    }
                 }
                 p += c;
             }
@@ -596,7 +657,7 @@ __device__ __forceinline__ double state_energy(const ProblemDev *PD, const int8_
     return e;
 }
 
-template <bool GIBBS, bool RANDOM_ORDER>
+template <bool GIBBS, bool RANDOM_ORDER, int S>
 __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *src,
                                             int8_t *dst, double *energy_out,
                                             double *de, int8_t *sp,
@@ -609,7 +670,7 @@ __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *
         if (RANDOM_ORDER)
             sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
         else
-            sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
+            sweep_sequential<GIBBS, S>(P, de, sp, scratch, ring, rs, lane, cnt);
     }
     __syncwarp();
     const double e = state_energy(PD, sp, lane);

@@ -10,7 +10,7 @@
 
 namespace b200sa {
 
-template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
+template <bool GIBBS, bool RANDOM_ORDER, bool SMEM, int S>
 __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
     sa_warp_kernel(LaunchArgs A, int warps_per_cta, int region_bytes) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -64,8 +64,9 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
         }
         const int64_t so = PD->state_offset + (int64_t)r * PD->n;
         Counters cnt = {0ull, 0ull, 0u};
-        anneal_read<GIBBS, RANDOM_ORDER>(PD, A.states_in + so, A.states_out + so,
-                                         &A.energies[rd], de, sp, scratch, ring, rs, lane, cnt);
+        anneal_read<GIBBS, RANDOM_ORDER, S>(PD, A.states_in + so, A.states_out + so,
+                                            &A.energies[rd], de, sp, scratch, ring, rs, lane,
+                                            cnt);
         if (lane == 0) {
             A.stats[rd].flips = cnt.flips;
             A.stats[rd].passes = cnt.passes;
@@ -89,15 +90,21 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
 using KernelFn = void (*)(LaunchArgs, int, int);
 
 static KernelFn kernel_for(int variant) {
-    switch (variant & 7) {
-        case 0: return sa_warp_kernel<false, false, false>;
-        case 1: return sa_warp_kernel<true, false, false>;
-        case 2: return sa_warp_kernel<false, true, false>;
-        case 3: return sa_warp_kernel<true, true, false>;
-        case 4: return sa_warp_kernel<false, false, true>;
-        case 5: return sa_warp_kernel<true, false, true>;
-        case 6: return sa_warp_kernel<false, true, true>;
-        default: return sa_warp_kernel<true, true, true>;
+    switch (variant & 15) {
+        case 0: return sa_warp_kernel<false, false, false, 1>;
+        case 1: return sa_warp_kernel<true, false, false, 1>;
+        case 2: return sa_warp_kernel<false, true, false, 1>;
+        case 3: return sa_warp_kernel<true, true, false, 1>;
+        case 4: return sa_warp_kernel<false, false, true, 1>;
+        case 5: return sa_warp_kernel<true, false, true, 1>;
+        case 6: return sa_warp_kernel<false, true, true, 1>;
+        case 7: return sa_warp_kernel<true, true, true, 1>;
+        // 64-variable windows (sequential order only)
+        case 8: return sa_warp_kernel<false, false, false, 2>;
+        case 9: return sa_warp_kernel<true, false, false, 2>;
+        case 12: return sa_warp_kernel<false, false, true, 2>;
+        case 13: return sa_warp_kernel<true, false, true, 2>;
+        default: return nullptr;
     }
 }
 
@@ -169,6 +176,7 @@ cudaError_t upload_jump_table(const uint32_t table[][4], cudaStream_t stream) {
 cudaError_t launch_sa(int variant, const LaunchArgs &args, int grid, int warps_per_cta,
                       int region_bytes, cudaStream_t stream) {
     const KernelFn k = kernel_for(variant);
+    if (!k) return cudaErrorInvalidValue;
     const size_t smem = (size_t)warps_per_cta * (size_t)region_bytes;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -178,6 +186,7 @@ cudaError_t launch_sa(int variant, const LaunchArgs &args, int grid, int warps_p
 
 cudaError_t kernel_occupancy(int variant, int warps_per_cta, int region_bytes, int *ctas_per_sm) {
     const KernelFn k = kernel_for(variant);
+    if (!k) return cudaErrorInvalidValue;
     const size_t smem = (size_t)warps_per_cta * (size_t)region_bytes;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

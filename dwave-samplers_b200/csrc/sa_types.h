@@ -19,11 +19,12 @@ constexpr int kPerLane = kHalf / 32;
 //   x          : start of the variable's adjacency list
 //   y bits 0-23: degree (list length)
 //   y bits 24-31: distance to the nearest later neighbour (u - v for the
-//                smallest neighbour u > v), capped at 32.  A flip of v can
-//                only change the decision of a variable inside the current
-//                32-wide window if that variable is at least this far ahead.
+//                smallest neighbour u > v), capped at kDistCap.  A flip of v
+//                can only change the decision of a variable inside the
+//                current window if that variable is at least this far ahead.
 constexpr uint32_t kDegMask = 0x00ffffffu;
 constexpr int kDistShift = 24;
+constexpr uint32_t kDistCap = 64;  // the widest speculative window
 constexpr uint32_t kMaxDegree = kDegMask;
 
 struct ProblemDev {
@@ -37,9 +38,9 @@ struct ProblemDev {
     const uint2 *vinfo;     // [n] per-variable record (see above)
     const uint8_t *dist;    // [n] the record's distance field alone (compact, L1-resident)
     // [n] conflict mask: bit 0 set when v's list names a target twice; bit j
-    // (1..31) set when v and v + j have a common neighbour.  Two committed
+    // (1..63) set when v and v + j have a common neighbour.  Two committed
     // flips can add into the same slot only through one of these.
-    const uint32_t *share;
+    const unsigned long long *share;
     const int32_t *col;     // [2m] neighbour index, coupler input order
     const double *w;        // [2m] coupling
     const double *h;        // [n]
@@ -93,9 +94,10 @@ constexpr int kJumpTable = kJumpNibbles * 16;
 constexpr int kCarryLaneWords = 64;                 // 32 lanes x 2 words
 constexpr int kCarryWords = kRing + kCarryLaneWords + 2;  // ring, lanes, q, base
 
-// Per-warp shared region: RNG ring, conflict scratch (32 doubles + 32 lane
-// indices), delta energies, spins.
-constexpr int kScratchBytes = 32 * 8 + 32 * 4;
+// Per-warp shared region: RNG ring, scratch (32 doubles for equal-slot sums,
+// 64 ints for the rank table of accepted flips), delta energies, spins.
+// (region_bytes_for keeps every region a multiple of 16 bytes.)
+constexpr int kScratchBytes = 32 * 8 + 64 * 4;
 inline int region_bytes_for(int cap_n) {
     const int spins = (cap_n + 15) & ~15;
     return kRing * 8 + kScratchBytes + cap_n * 8 + spins;

@@ -70,6 +70,7 @@ typedef struct {
     int64_t near_ties;    /* exp() decisions inside the cross-libm tie band */
     int64_t passes;       /* warp passes of the sequential sweep (speculation efficiency) */
     double kernel_ms;     /* device time of the sampling launches (CUDA events) */
+    int64_t launches;     /* sweep-kernel launches issued */
 } b200sa_stats;
 
 /* One binary quadratic model in Ising form plus its reads.
@@ -144,6 +145,27 @@ B200SA_API int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_s
                     b200sa_stats *stats, char *err, size_t errlen);
 
 B200SA_API int b200sa_plan_destroy(b200sa_plan plan);
+
+/* ---- Sample moments (no reference counterpart) ------------------------------
+ * For the gradient of log Z of p(s) ~ exp(-beta*E(s)), E as in cpu_sa.cpp:210-227:
+ * d log Z/d h_i = -beta <s_i>, d log Z/d J_c = -beta <s_u(c) s_v(c)>.  Adds the
+ * exact integer sums over reads of s_i (sum_s) and of s_u*s_v per coupler in COO
+ * order (sum_ss) to the caller's zero-initialised device arrays, for many
+ * problems in one launch.  All pointers are device memory; coupler indices
+ * must be valid (num_vars <= 4096). */
+typedef struct {
+    int32_t num_vars;
+    int64_t num_couplers;
+    int32_t num_reads;
+    const int8_t *states;           /* [num_reads * num_vars] */
+    const int32_t *coupler_starts;  /* [num_couplers] */
+    const int32_t *coupler_ends;    /* [num_couplers] */
+    int64_t *sum_s;                 /* [num_vars], accumulated into */
+    int64_t *sum_ss;                /* [num_couplers], accumulated into */
+} b200sa_moments_problem;
+
+B200SA_API int b200sa_edge_moments(const b200sa_moments_problem *problems, int32_t num_problems,
+                                   int32_t device, void *stream, char *err, size_t errlen);
 
 /* No counterpart in the reference.  The sampler for callers that cannot
  * allocate device memory while they run (all device memory owned by a
