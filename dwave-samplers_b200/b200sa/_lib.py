@@ -26,6 +26,8 @@ RANDOM = 1
 
 MODE_PERSISTENT = 0
 MODE_PLAIN = 1
+MODE_GRAPH = 2
+TUNE_FORCE = 1
 
 EXPORTS = (
     "b200sa_sample",
@@ -38,6 +40,9 @@ EXPORTS = (
     "b200sa_check_acceptance",
     "b200sa_sample_noalloc",
     "b200sa_edge_moments",
+    "b200sa_random_states",
+    "b200sa_plan_set_weights",
+    "b200sa_plan_autotune",
 )
 
 
@@ -89,6 +94,24 @@ class MomentsProblem(ctypes.Structure):
     ]
 
 
+class TuneEntry(ctypes.Structure):
+    _fields_ = [
+        ("bucket", ctypes.c_int32),
+        ("kind", ctypes.c_int32),
+        ("max_n", ctypes.c_int32),
+        ("items", ctypes.c_int64),
+        ("onchip", ctypes.c_int32),
+        ("warps_per_cta", ctypes.c_int32),
+        ("ctas_per_sm", ctypes.c_int32),
+        ("attempts_per_s", ctypes.c_double),
+        ("from_cache", ctypes.c_int32),
+        ("candidates", ctypes.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 INTERRUPT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
 
 _lib = None
@@ -137,6 +160,15 @@ def load() -> ctypes.CDLL:
     L.b200sa_edge_moments.restype = c.c_int
     L.b200sa_edge_moments.argtypes = [c.POINTER(MomentsProblem), c.c_int32, c.c_int32,
                                       c.c_void_p, c.c_char_p, c.c_size_t]
+    L.b200sa_random_states.restype = c.c_int
+    L.b200sa_random_states.argtypes = [c.c_uint64, c.c_uint64, c.c_int64, c.c_int64, c.c_int32,
+                                       c.c_void_p, c.c_int32, c.c_void_p, c.c_char_p, c.c_size_t]
+    L.b200sa_plan_set_weights.restype = c.c_int
+    L.b200sa_plan_set_weights.argtypes = [c.c_void_p, c.c_int32, c.c_void_p, c.c_void_p,
+                                          c.c_char_p, c.c_size_t]
+    L.b200sa_plan_autotune.restype = c.c_int
+    L.b200sa_plan_autotune.argtypes = [c.c_void_p, c.c_char_p, c.c_int32, c.POINTER(TuneEntry),
+                                       c.c_int32, c.c_char_p, c.c_size_t]
     L.b200sa_version.restype = c.c_char_p
     L.b200sa_version.argtypes = []
     _lib = L

@@ -69,36 +69,95 @@ def initial_states(init_seed: int, model_index: int, reads: int, n: int,
     return np.where((x >> np.uint64(63)) != 0, 1, -1).astype(np.int8)
 
 
+def device_initial_states(out: torch.Tensor, init_seed: int, model_index: int, read0: int,
+                          reads: int, n: int, device: int = 0) -> torch.Tensor:
+    """:func:`initial_states` generated on the GPU into ``out`` (int8 CUDA
+    tensor of reads * n elements) by ``b200sa_random_states``."""
+    if out.dtype != torch.int8 or not out.is_cuda or out.numel() != reads * n:
+        raise ValueError("out must be an int8 CUDA tensor of reads * n elements")
+    err = _lib.errbuf()
+    rc = _lib.load().b200sa_random_states(
+        int(init_seed), int(model_index), int(read0), int(reads), int(n), out.data_ptr(),
+        int(device), torch.cuda.current_stream(out.device).cuda_stream, err, len(err))
+    _lib.check(rc, err)
+    return out
+
+
 def read_seeds(seed: int, model_index: int, reads: int, read0: int = 0) -> np.ndarray:
     base = (np.uint64(seed) * np.uint64(1000003) + np.uint64(model_index) * np.uint64(1 << 40))
     with np.errstate(over="ignore"):
         return base + np.arange(read0, read0 + reads, dtype=np.uint64)
 
 
+class ModelSampler:
+    """Fixed-beta sampling of a fixed set of model structures.
+
+    The models are packed into one plan once; every call writes the new
+    fields and couplings into it (``b200sa_plan_set_weights``), generates the
+    initial states on the GPU, uploads the per-read seeds and replays the
+    plan's captured CUDA graph over the same device buffers.  Reads
+    [read0, read0 + reads) of model k start from ``initial_states(init_seed,
+    k, reads, n, read0)`` with seeds ``read_seeds(seed, k, reads, read0)``.
+    """
+
+    def __init__(self, models: Sequence[IsingModel], beta: float, sweeps: int, reads: int,
+                 proposal: str = "Gibbs", device: int = 0):
+        self.models = list(models)
+        self.reads = int(reads)
+        self.device = int(device)
+        dev = torch.device("cuda", self.device)
+        insts = [Instance(
+            np.zeros(m.num_vars), m.u, m.v, np.zeros(m.num_couplers),
+            # shape only: the plan packs structure, the states are made on the GPU
+            np.broadcast_to(np.zeros(1, np.int8), (self.reads, m.num_vars)),
+            np.array([float(beta)]), int(sweeps), np.zeros(self.reads, np.uint64),
+            proposal=proposal) for m in self.models]
+        self.plan = Plan(insts, device=self.device)
+        self.sin = torch.empty(max(self.plan.total_state, 1), dtype=torch.int8, device=dev)
+        self.sout = torch.empty_like(self.sin)
+        self.en = torch.empty(max(self.plan.total_reads, 1), dtype=torch.float64, device=dev)
+        self.seeds = torch.empty(max(self.plan.total_reads, 1), dtype=torch.int64, device=dev)
+
+    def sample(self, hs, Js, seed: int, init_seed: int, read0: int = 0) -> list[torch.Tensor]:
+        """One int8 CUDA tensor (reads x n) per model; the tensors are views of
+        the sampler's output buffer, overwritten by the next call."""
+        dev = self.sin.device
+        offs = self.plan.state_offsets
+        for k, (h, J) in enumerate(zip(hs, Js)):
+            self.plan.set_weights(k, h, J)
+        seeds = np.concatenate([read_seeds(seed, k, self.reads, read0)
+                                for k in range(len(self.models))])
+        self.seeds[:seeds.shape[0]].copy_(torch.from_numpy(seeds.view(np.int64)))
+        for k, mod in enumerate(self.models):
+            device_initial_states(self.sin[int(offs[k]):int(offs[k + 1])], init_seed, k, read0,
+                                  self.reads, mod.num_vars, self.device)
+        self.plan.run(self.sin, self.sout, self.en, seeds=self.seeds, mode="graph",
+                      stream=torch.cuda.current_stream(dev), sync=True)
+        return [self.sout[int(offs[k]):int(offs[k + 1])].view(self.reads, m.num_vars)
+                for k, m in enumerate(self.models)]
+
+    def close(self):
+        self.plan.close()
+
+
 def sample_models(models: Sequence[IsingModel], hs: Sequence[np.ndarray],
                   Js: Sequence[np.ndarray], beta: float, sweeps: int, reads: int,
                   seed: int, init_seed: int, read0: int = 0, proposal: str = "Gibbs",
-                  device: int = 0) -> list[torch.Tensor]:
+                  device: int = 0, sampler: ModelSampler | None = None) -> list[torch.Tensor]:
     """Fixed-beta sampling of every model (one persistent batch): reads
     [read0, read0 + reads) of each model, `sweeps` sweeps at `beta`.
-    Returns one int8 CUDA tensor (reads x n) per model."""
-    insts = []
-    for k, (mod, h, J) in enumerate(zip(models, hs, Js)):
-        insts.append(Instance(
-            np.ascontiguousarray(h, dtype=np.float64), mod.u, mod.v,
-            np.ascontiguousarray(J, dtype=np.float64),
-            initial_states(init_seed, k, reads, mod.num_vars, read0),
-            np.array([float(beta)]), int(sweeps), read_seeds(seed, k, reads, read0),
-            proposal=proposal))
-    dev = torch.device("cuda", device)
-    with Plan(insts, device=device) as plan:
-        host = np.concatenate([p.states.ravel() for p in insts])
-        sin = torch.from_numpy(host).to(dev)
-        sout = torch.empty_like(sin)
-        en = torch.empty(plan.total_reads, dtype=torch.float64, device=dev)
-        plan.run(sin, sout, en, stream=torch.cuda.current_stream(dev), sync=True)
-        offs = plan.state_offsets
-    return [sout[int(offs[k]):int(offs[k + 1])].view(reads, insts[k].n) for k in range(len(insts))]
+    Returns one int8 CUDA tensor (reads x n) per model.  With `sampler` (a
+    :class:`ModelSampler` built for these models, reads and settings) its
+    plan and graph are reused; the results are the same."""
+    own = sampler is None
+    if own:
+        sampler = ModelSampler(models, beta, sweeps, reads, proposal, device)
+    try:
+        out = sampler.sample(hs, Js, seed, init_seed, read0)
+        return [x.clone() for x in out] if not own else out
+    finally:
+        if own:
+            sampler.close()
 
 
 def edge_moments(models: Sequence[IsingModel], samples: Sequence[torch.Tensor],
@@ -154,7 +213,8 @@ class LogPartition(torch.autograd.Function):
         samples = []
         if keep:
             samples = sample_models(spec.models, hs, Js, spec.beta, spec.sweeps, spec.reads,
-                                    spec.seed, spec.init_seed, 0, spec.proposal, spec.device)
+                                    spec.seed, spec.init_seed, 0, spec.proposal, spec.device,
+                                    spec.sampler(spec.reads))
         spec.last_samples = samples
         ctx.spec = spec
         ctx.hs, ctx.Js = hs, Js
@@ -188,6 +248,17 @@ class SamplingSpec:
     device: int = 0
     last_samples: list = None      # set by LogPartition.forward
     last_moments: tuple = None     # set by LogPartition.backward
+    samplers: dict = None          # reads per call -> ModelSampler (plan + graph reused)
+
+    def sampler(self, reads: int) -> ModelSampler:
+        """The spec's sampler for calls of `reads` reads (built on first use;
+        later calls reuse its plan and captured graph)."""
+        if self.samplers is None:
+            self.samplers = {}
+        if reads not in self.samplers:
+            self.samplers[reads] = ModelSampler(self.models, self.beta, self.sweeps, reads,
+                                                self.proposal, self.device)
+        return self.samplers[reads]
 
     def split(self, h_cat, J_cat):
         hs, Js, i, j = [], [], 0, 0
@@ -206,7 +277,8 @@ class SamplingSpec:
         for r0 in range(0, self.reads, self.recompute_chunk):
             k = min(self.recompute_chunk, self.reads - r0)
             chunk = sample_models(self.models, hs, Js, self.beta, self.sweeps, k, self.seed,
-                                  self.init_seed, r0, self.proposal, self.device)
+                                  self.init_seed, r0, self.proposal, self.device,
+                                  self.sampler(k))
             s, ss = edge_moments(self.models, chunk, self.device)
             if tot_s is None:
                 tot_s, tot_ss = s, ss

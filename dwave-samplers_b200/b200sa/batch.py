@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from .workloads import Instance
 
-MODES = {"persistent": _lib.MODE_PERSISTENT, "plain": _lib.MODE_PLAIN}
+MODES = {"persistent": _lib.MODE_PERSISTENT, "plain": _lib.MODE_PLAIN, "graph": _lib.MODE_GRAPH}
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 
 
@@ -138,6 +138,29 @@ class Plan:
                                        1 if sync else 0, ctypes.byref(st), err, len(err))
         _lib.check(rc, err)
         return st.as_dict()
+
+    def set_weights(self, problem: int, h, J):
+        """Replace problem ``problem``'s fields and coupler weights (COO order
+        as given at creation); structure, schedule and seeds are kept."""
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        J = np.ascontiguousarray(J, dtype=np.float64)
+        err = _lib.errbuf()
+        rc = self._lib.b200sa_plan_set_weights(self.handle, int(problem), h.ctypes.data,
+                                               J.ctypes.data, err, len(err))
+        _lib.check(rc, err)
+
+    def autotune(self, cache_path: str | None = None, force: bool = False) -> list[dict]:
+        """Measure launch configurations per size bucket and keep the fastest
+        for persistent / graph runs (results are unchanged).  Choices are
+        cached in ``cache_path``.  Returns one dict per non-empty bucket."""
+        cap = 64
+        rep = (_lib.TuneEntry * cap)()
+        err = _lib.errbuf()
+        path = cache_path.encode() if cache_path else None
+        rc = self._lib.b200sa_plan_autotune(self.handle, path, _lib.TUNE_FORCE if force else 0,
+                                            rep, cap, err, len(err))
+        _lib.check(rc, err)
+        return [rep[i].as_dict() for i in range(min(rc, cap))]
 
     def close(self):
         if self.handle:

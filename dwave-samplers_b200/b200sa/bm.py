@@ -67,11 +67,14 @@ def fit(truth: Sequence[tuple], beta: float = 1.0, steps: int = 500, reads: int 
     h_cat = torch.from_numpy(np.concatenate(hs)).to(dev)
     J = torch.zeros(data.shape[0], dtype=torch.float64, device=dev, requires_grad=True)
     opt = torch.optim.Adam([J], lr=lr)
+    samplers = None  # one plan and graph for every step
     for step in range(steps):
         t = time.perf_counter()
         spec = SamplingSpec(models, beta=beta, sweeps=sweeps, reads=reads,
-                            seed=seed + 1000 + step, init_seed=seed + 7 + step, device=device)
+                            seed=seed + 1000 + step, init_seed=seed + 7 + step, device=device,
+                            samplers=samplers)
         loss = beta * torch.dot(J, data) + log_partition(h_cat, J, spec)
+        samplers = spec.samplers
         opt.zero_grad()
         loss.backward()
         opt.step()

@@ -87,9 +87,10 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
         out.col[k] = a;
         out.w[k] = J;
     }
-    // Speculation info: nearest later neighbour; repeated targets; pairs of
-    // variables less than 64 apart with a common neighbour.
-    out.share.assign((size_t)n, 0ull);
+    // Speculation record: nearest later neighbour; repeated targets; pairs
+    // of variables less than 32 apart with a common neighbour.
+    out.share.assign((size_t)n, 0u);
+    out.dist.assign((size_t)n, 0u);
     {
         std::vector<int32_t> nb;
         for (int32_t u = 0; u < n; ++u) {
@@ -97,8 +98,8 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
             std::sort(nb.begin(), nb.end());
             nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
             for (size_t i = 0; i < nb.size(); ++i)
-                for (size_t j = i + 1; j < nb.size() && nb[j] - nb[i] < 64; ++j)
-                    out.share[nb[i]] |= 1ull << (nb[j] - nb[i]);
+                for (size_t j = i + 1; j < nb.size() && nb[j] - nb[i] < 32; ++j)
+                    out.share[nb[i]] |= 1u << (nb[j] - nb[i]);
         }
     }
     std::vector<int32_t> mark((size_t)n, -1);
@@ -113,12 +114,13 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
             if (u > v) dist = std::min<uint32_t>(dist, (uint32_t)(u - v));
             if (mark[u] == v) {
                 any_dup = true;
-                out.share[v] |= 1ull;
+                out.share[v] |= 1u;
             }
             mark[u] = v;
         }
         out.vinfo[2 * (size_t)v] = (uint32_t)e0;
-        out.vinfo[2 * (size_t)v + 1] = (uint32_t)(e1 - e0) | (dist << kDistShift);
+        out.vinfo[2 * (size_t)v + 1] = (uint32_t)(e1 - e0);
+        out.dist[v] = (uint8_t)dist;
     }
     out.max_degree = maxdeg;
     out.any_dup = any_dup;

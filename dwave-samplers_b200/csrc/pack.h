@@ -12,8 +12,9 @@ struct PackedAdjacency {
     std::vector<int32_t> row;     // n+1
     std::vector<int32_t> col;     // 2m
     std::vector<double> w;        // 2m
-    std::vector<uint32_t> vinfo;  // 2n: per variable {list start, degree | dist << 24}
-    std::vector<uint64_t> share;  // n: conflict mask (see ProblemDev::share)
+    std::vector<uint32_t> vinfo;  // 2n: per variable {list start, degree}
+    std::vector<uint8_t> dist;    // n: speculation distance (ProblemDev::dist)
+    std::vector<uint32_t> share;  // n: conflict mask (ProblemDev::share)
     int32_t max_degree = 0;
     int32_t regular_degree = 0;   // common list length when all lists are equally long
     bool any_dup = false;         // some list names a target twice (self-loop / repeat)

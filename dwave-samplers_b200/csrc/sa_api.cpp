@@ -21,36 +21,13 @@
 #include "sa_launch.h"
 #include "sa_types.h"
 
+#include "plan.h"
+
 using namespace b200sa;
+using namespace b200sa::host;
 
-namespace {
-
-int set_err(char *err, size_t errlen, int code, const std::string &msg) {
-    if (err && errlen > 0) std::snprintf(err, errlen, "%s", msg.c_str());
-    return code;
-}
-
-#define B200SA_CUDA(call)                                                        \
-    do {                                                                         \
-        cudaError_t e_ = (call);                                                 \
-        if (e_ != cudaSuccess)                                                   \
-            return set_err(err, errlen, B200SA_ECUDA,                            \
-                           std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-// Restores the caller's current device on scope exit.
-struct DeviceGuard {
-    int prev = -1;
-    DeviceGuard() {
-        if (cudaGetDevice(&prev) != cudaSuccess) {
-            prev = -1;
-            cudaGetLastError();
-        }
-    }
-    ~DeviceGuard() {
-        if (prev >= 0) cudaSetDevice(prev);
-    }
-};
+namespace b200sa {
+namespace host {
 
 int select_device(int device, cudaDeviceProp &prop, char *err, size_t errlen) {
     int count = 0;
@@ -70,28 +47,6 @@ int select_device(int device, cudaDeviceProp &prop, char *err, size_t errlen) {
     return B200SA_OK;
 }
 
-template <typename T>
-struct DevArray {
-    T *ptr = nullptr;
-    size_t count = 0;
-    DevArray() = default;
-    DevArray(const DevArray &) = delete;
-    DevArray &operator=(const DevArray &) = delete;
-    ~DevArray() { release(); }
-    void release() {
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        count = 0;
-    }
-    cudaError_t alloc(size_t n) {
-        release();
-        count = n;
-        if (n == 0) return cudaSuccess;
-        return cudaMalloc(reinterpret_cast<void **>(&ptr), n * sizeof(T));
-    }
-};
-
-size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 const uint32_t (*jump_table())[4] {
     static uint32_t table[kJumpTable][4];
@@ -103,92 +58,6 @@ const uint32_t (*jump_table())[4] {
     });
     return table;
 }
-
-// Buckets of the persistent mode: a size class crossed with the kernel kind
-// (acceptance rule x update order).  Each bucket's warps get a shared region
-// sized for the bucket's largest n, so small problems pack more resident
-// warps per SM; the last size class keeps its state in global memory.
-constexpr int kSizeClasses = 8;
-constexpr int kGlobalClass = kSizeClasses - 1;
-constexpr int kKinds = 8;
-constexpr int kBuckets = kSizeClasses * kKinds;
-constexpr int kStreams = 8;
-const int kClassBound[kSizeClasses - 2] = {128, 256, 512, 1024, 2048, 4096};
-
-int size_class(int n, int onchip_max) {
-    if (n > onchip_max) return kGlobalClass;
-    for (int b = 0; b < kSizeClasses - 2; ++b)
-        if (n <= kClassBound[b]) return b;
-    return kSizeClasses - 2;
-}
-
-// Kernel kind of a problem: bit 0 Gibbs, bit 1 random order, bit 2 wide
-// (64-variable) windows.  Wide windows need equal-length lists; measured on
-// the random-regular shapes of the benchmark (n 500-4000, degree 6-16) they
-// raise attempts per pass by ~40% but the extra update round costs as much,
-// so they are not selected by default.
-bool wide_windows(const ProblemDev &d, bool allow_wide) {
-    return allow_wide && d.varorder == 0 && d.regular_degree > 0;
-}
-
-int kind_of(const ProblemDev &d, bool allow_wide = false) {
-    return (d.proposal == 0 ? 1 : 0) | (d.varorder ? 2 : 0) | (wide_windows(d, allow_wide) ? 4 : 0);
-}
-
-}  // namespace
-
-struct b200sa_plan_s {
-    int device = 0;
-    cudaDeviceProp prop{};
-    cudaStream_t stream = nullptr;
-    cudaStream_t bstream[kStreams] = {};
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
-    cudaEvent_t join[kStreams] = {};
-    int num_problems = 0;
-    int onchip_max = 0;
-    std::vector<ProblemDev> hprobs;
-    std::vector<int32_t> n, reads, sweeps;  // per problem
-    std::vector<int64_t> state_off, read_off;
-    int64_t total_state = 0, total_reads = 0;
-    int32_t max_n = 0;
-    DevArray<uint8_t> arena;
-    DevArray<ProblemDev> dprobs;
-    DevArray<uint64_t> dseeds;
-    DevArray<ReadStats> dstats;
-    DevArray<int64_t> items_lpt, items_plain;
-    DevArray<unsigned long long> qhead;  // one per bucket
-    DevArray<double> scratch_de;
-    DevArray<int8_t> scratch_s;
-    DevArray<uint64_t> carry;
-    int64_t scratch_stride = 0, scratch_slots = 0;
-    std::vector<int64_t> plain_item_off;   // per problem offset into items_plain
-    int64_t bucket_off[kBuckets + 1] = {};  // bucket ranges in items_lpt
-    int32_t bucket_max_n[kBuckets] = {};
-    int64_t bucket_lead_cost[kBuckets] = {};
-    std::map<std::pair<int, int>, int> occ_cache;  // (variant*2^24 + warps, region) -> CTAs/SM
-    int64_t launches = 0;  // sweep-kernel launches issued by the current run
-
-    ~b200sa_plan_s() {
-        if (ev0) cudaEventDestroy(ev0);
-        if (ev1) cudaEventDestroy(ev1);
-        if (fork) cudaEventDestroy(fork);
-        for (int b = 0; b < kStreams; ++b) {
-            if (join[b]) cudaEventDestroy(join[b]);
-            if (bstream[b]) cudaStreamDestroy(bstream[b]);
-        }
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
-
-namespace {
-
-struct LaunchShape {
-    int cap_n;         // largest n kept in shared memory
-    int warps_per_cta;
-    int region;
-    int grid;
-    int variant;
-};
 
 int occupancy(b200sa_plan_s *P, int variant, int w, int region, int *ctas, char *err,
               size_t errlen) {
@@ -208,11 +77,30 @@ int occupancy(b200sa_plan_s *P, int variant, int w, int region, int *ctas, char 
 // and spins (else those live in a global slot, L2-resident).  Warps per CTA
 // are chosen to maximize resident warps per SM.
 int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, bool persistent,
-              LaunchShape &out, char *err, size_t errlen) {
+              LaunchShape &out, char *err, size_t errlen, const TuneChoice *choice) {
     const int smem_blk = (int)P->prop.sharedMemPerBlockOptin;
-    const int cap = max_n_here <= P->onchip_max ? max_n_here : 0;
+    const bool onchip = choice && choice->set ? choice->onchip : true;
+    const int cap = onchip && max_n_here <= P->onchip_max ? max_n_here : 0;
     const int region = region_bytes_for(cap);
-    const int variant = kernel_variant(kind & 1, kind & 2, cap > 0, kind & 4);
+    const int variant = kernel_variant(kind & 1, kind & 2, cap > 0);
+    if (choice && choice->set && persistent) {
+        // The autotuner's measured configuration.
+        const int w = choice->warps_per_cta;
+        if (w < 1 || w > kMaxThreadsPerCta / 32 || (int64_t)w * region > smem_blk)
+            return set_err(err, errlen, B200SA_EINVAL, "tuned shape does not fit");
+        int ctas = 0;
+        int rc = occupancy(P, variant, w, region, &ctas, err, errlen);
+        if (rc) return rc;
+        if (ctas < 1) return set_err(err, errlen, B200SA_ECUDA, "tuned shape does not fit on an SM");
+        if (choice->ctas_per_sm > 0) ctas = std::min(ctas, choice->ctas_per_sm);
+        out.cap_n = cap;
+        out.warps_per_cta = w;
+        out.region = region;
+        out.grid = (int)std::max<int64_t>(
+            1, std::min<int64_t>((int64_t)P->prop.multiProcessorCount * ctas, (items + w - 1) / w));
+        out.variant = variant;
+        return B200SA_OK;
+    }
     int best_w = 1, best_warps = 0;
     for (int w = 1; w <= kMaxThreadsPerCta / 32; ++w) {
         if ((int64_t)w * region > smem_blk) break;
@@ -254,6 +142,13 @@ int ensure_scratch(b200sa_plan_s *P, int64_t slots, int64_t stride, char *err,
     if (slots <= P->scratch_slots && stride <= P->scratch_stride) return B200SA_OK;
     slots = std::max(slots, P->scratch_slots);
     stride = std::max(stride, P->scratch_stride);
+    // The old slots may still be in use by an enqueued run, and a captured
+    // graph holds their addresses.
+    B200SA_CUDA(cudaDeviceSynchronize());
+    if (P->graph_exec) {
+        cudaGraphExecDestroy(P->graph_exec);
+        P->graph_exec = nullptr;
+    }
     B200SA_CUDA(P->scratch_de.alloc((size_t)(slots * stride)));
     B200SA_CUDA(P->scratch_s.alloc((size_t)(slots * stride)));
     P->scratch_slots = slots;
@@ -275,33 +170,58 @@ LaunchArgs base_args(b200sa_plan_s *P, const int8_t *in, int8_t *out, double *en
 
 // One launch over `count` items.  Persistent launches take items from the
 // work-queue head `qhead` (zeroed by the caller, stream-ordered).
-int launch_items(b200sa_plan_s *P, LaunchArgs a, int kind, const int64_t *items,
-                 int64_t count, int32_t max_n_here, bool persistent, bool shared_stream,
-                 unsigned long long *qhead, cudaStream_t st, char *err, size_t errlen) {
-    if (count <= 0) return B200SA_OK;
-    LaunchShape s{};
+int items_shape(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t count, bool persistent,
+                bool shared_stream, const TuneChoice *choice, LaunchShape &s, char *err,
+                size_t errlen) {
     int rc = shape_for(P, kind, max_n_here, shared_stream ? 1 : count,
-                       persistent && !shared_stream, s, err, errlen);
+                       persistent && !shared_stream, s, err, errlen,
+                       shared_stream ? nullptr : choice);
     if (rc) return rc;
-    if (shared_stream) {
+    if (shared_stream) {  // one stream continued read after read: one warp
         s.grid = 1;
         s.warps_per_cta = 1;
     }
+    return B200SA_OK;
+}
+
+int launch_shape(b200sa_plan_s *P, LaunchArgs a, const LaunchShape &s, const int64_t *items,
+                 int64_t count, int32_t max_n_here, bool persistent, bool shared_stream,
+                 unsigned long long *qhead, int64_t slot0, cudaStream_t st, char *err,
+                 size_t errlen) {
+    if (count <= 0) return B200SA_OK;
     if (max_n_here > s.cap_n) {
-        rc = ensure_scratch(P, (int64_t)s.grid * s.warps_per_cta, max_n_here, err, errlen);
-        if (rc) return rc;
+        const int64_t end = slot0 + (int64_t)s.grid * s.warps_per_cta;
+        if (end > P->scratch_slots || max_n_here > P->scratch_stride)
+            return set_err(err, errlen, B200SA_EINVAL, "internal: global slots not reserved");
+        a.scratch_de = P->scratch_de.ptr + slot0 * P->scratch_stride;
+        a.scratch_s = P->scratch_s.ptr + slot0 * P->scratch_stride;
+        a.scratch_stride = P->scratch_stride;
+        a.num_slots = end - slot0;
     }
     a.items = items;
     a.num_items = count;
     a.smem_cap_n = s.cap_n;
-    a.scratch_de = P->scratch_de.ptr;
-    a.scratch_s = P->scratch_s.ptr;
-    a.scratch_stride = P->scratch_stride;
-    a.num_slots = P->scratch_slots;
     a.queue_head = (persistent && !shared_stream) ? qhead : nullptr;
     B200SA_CUDA(launch_sa(s.variant, a, s.grid, s.warps_per_cta, s.region, st));
     P->launches++;
     return B200SA_OK;
+}
+
+int launch_items(b200sa_plan_s *P, LaunchArgs a, int kind, const int64_t *items,
+                 int64_t count, int32_t max_n_here, bool persistent, bool shared_stream,
+                 unsigned long long *qhead, cudaStream_t st, char *err, size_t errlen,
+                 const TuneChoice *choice) {
+    if (count <= 0) return B200SA_OK;
+    LaunchShape s{};
+    int rc = items_shape(P, kind, max_n_here, count, persistent, shared_stream, choice, s, err,
+                         errlen);
+    if (rc) return rc;
+    if (max_n_here > s.cap_n) {
+        rc = ensure_scratch(P, (int64_t)s.grid * s.warps_per_cta, max_n_here, err, errlen);
+        if (rc) return rc;
+    }
+    return launch_shape(P, a, s, items, count, max_n_here, persistent, shared_stream, qhead, 0,
+                        st, err, errlen);
 }
 
 int collect_stats(b200sa_plan_s *P, const std::vector<std::pair<int, int>> &ranges,
@@ -333,6 +253,29 @@ int collect_stats(b200sa_plan_s *P, const std::vector<std::pair<int, int>> &rang
 // as earlier ones drain.
 int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
                    size_t errlen) {
+    // Shapes first: the launches below may run at the same time, so those
+    // that keep their state in global slots get disjoint slot ranges.
+    LaunchShape shape[kBuckets];
+    int64_t slot0[kBuckets] = {};
+    int64_t slots = 0;
+    int32_t stride = 0;
+    for (int b = 0; b < kBuckets; ++b) {
+        const int64_t cnt = P->bucket_off[b + 1] - P->bucket_off[b];
+        if (cnt <= 0) continue;
+        int rc = items_shape(P, b % kKinds, P->bucket_max_n[b], cnt, true, false, &P->tune[b],
+                             shape[b], err, errlen);
+        if (rc) return rc;
+        if (P->bucket_max_n[b] > shape[b].cap_n) {
+            slot0[b] = slots;
+            slots += (int64_t)shape[b].grid * shape[b].warps_per_cta;
+            stride = std::max(stride, P->bucket_max_n[b]);
+        }
+    }
+    if (slots > 0) {
+        int rc = ensure_scratch(P, slots, stride, err, errlen);
+        if (rc) return rc;
+    }
+    if (P->dry_run) return B200SA_OK;
     B200SA_CUDA(cudaMemsetAsync(P->qhead.ptr, 0, sizeof(unsigned long long) * kBuckets, st));
     B200SA_CUDA(cudaEventRecord(P->fork, st));
     int order[kBuckets];
@@ -349,8 +292,8 @@ int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
         const int si = next++ % kStreams;
         if (!used[si]) B200SA_CUDA(cudaStreamWaitEvent(P->bstream[si], P->fork, 0));
         used[si] = true;
-        int rc = launch_items(P, a, b % kKinds, P->items_lpt.ptr + P->bucket_off[b], cnt,
-                              P->bucket_max_n[b], true, false, P->qhead.ptr + b,
+        int rc = launch_shape(P, a, shape[b], P->items_lpt.ptr + P->bucket_off[b], cnt,
+                              P->bucket_max_n[b], true, false, P->qhead.ptr + b, slot0[b],
                               P->bstream[si], err, errlen);
         if (rc) return rc;
     }
@@ -362,7 +305,8 @@ int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
     return B200SA_OK;
 }
 
-}  // namespace
+}  // namespace host
+}  // namespace b200sa
 
 extern "C" {
 
@@ -426,10 +370,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
 
     // Pack and lay out every problem in one device arena.
     std::vector<PackedAdjacency> adj((size_t)num_problems);
-    struct Off {
-        size_t vinfo, dist, share, col, w, h, cu, cv, cw, betas, thr;
-    };
-    std::vector<Off> off((size_t)num_problems);
+    std::vector<ArenaOffsets> off((size_t)num_problems);
     size_t bytes = 0;
     auto take = [&](size_t sz) {
         const size_t o = bytes;
@@ -443,10 +384,10 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         pack_adjacency(q, adj[i]);
         const size_t n = (size_t)q.num_vars, m = (size_t)q.num_couplers,
                      nb = (size_t)q.num_betas;
-        Off &o = off[i];
+        ArenaOffsets &o = off[i];
         o.vinfo = take(8 * n);
         o.dist = take(n);
-        o.share = take(8 * n);
+        o.share = take(4 * n);
         o.col = take(4 * 2 * m);
         o.w = take(8 * 2 * m);
         o.h = take(8 * n);
@@ -467,7 +408,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
     std::vector<uint8_t> staging(bytes);
     for (int32_t i = 0; i < num_problems; ++i) {
         const b200sa_problem &q = problems[i];
-        const Off &o = off[i];
+        const ArenaOffsets &o = off[i];
         const size_t n = (size_t)q.num_vars, m = (size_t)q.num_couplers,
                      nb = (size_t)q.num_betas;
         if (m) {
@@ -479,9 +420,8 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         }
         if (n) {
             std::memcpy(&staging[o.vinfo], adj[i].vinfo.data(), 8 * n);
-            for (size_t v = 0; v < n; ++v)
-                staging[o.dist + v] = (uint8_t)(adj[i].vinfo[2 * v + 1] >> kDistShift);
-            std::memcpy(&staging[o.share], adj[i].share.data(), 8 * n);
+            std::memcpy(&staging[o.dist], adj[i].dist.data(), n);
+            std::memcpy(&staging[o.share], adj[i].share.data(), 4 * n);
             std::memcpy(&staging[o.h], q.h, 8 * n);
         }
         if (nb) {
@@ -495,10 +435,13 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
     if (bytes)
         B200SA_CUDA(cudaMemcpyAsync(P->arena.ptr, staging.data(), bytes,
                                     cudaMemcpyHostToDevice, P->stream));
+    P->offs = off;
+    P->rows.resize((size_t)num_problems);
+    for (int32_t i = 0; i < num_problems; ++i) P->rows[i] = std::move(adj[i].row);
     P->hprobs.resize((size_t)num_problems);
     for (int32_t i = 0; i < num_problems; ++i) {
         const b200sa_problem &q = problems[i];
-        const Off &o = off[i];
+        const ArenaOffsets &o = off[i];
         ProblemDev &d = P->hprobs[i];
         uint8_t *base = P->arena.ptr;
         d.n = q.num_vars;
@@ -510,7 +453,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         d.read_offset = P->read_off[i];
         d.vinfo = reinterpret_cast<const uint2 *>(base + o.vinfo);
         d.dist = base + o.dist;
-        d.share = reinterpret_cast<const unsigned long long *>(base + o.share);
+        d.share = reinterpret_cast<const uint32_t *>(base + o.share);
         d.col = reinterpret_cast<const int32_t *>(base + o.col);
         d.w = reinterpret_cast<const double *>(base + o.w);
         d.h = reinterpret_cast<const double *>(base + o.h);
@@ -588,6 +531,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
     }
     B200SA_CUDA(upload_jump_table(jump_table(), P->stream));
     B200SA_CUDA(cudaStreamSynchronize(P->stream));
+    P->h_items_lpt = std::move(lpt);
     *out = P.release();
     return B200SA_OK;
 }
@@ -615,7 +559,7 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
                     void *stream, int32_t sync, b200sa_stats *stats, char *err,
                     size_t errlen) {
     if (!plan) return set_err(err, errlen, B200SA_EINVAL, "plan is NULL");
-    if (mode != B200SA_MODE_PERSISTENT && mode != B200SA_MODE_PLAIN)
+    if (mode != B200SA_MODE_PERSISTENT && mode != B200SA_MODE_PLAIN && mode != B200SA_MODE_GRAPH)
         return set_err(err, errlen, B200SA_EINVAL, "unknown mode");
     if (plan->total_reads > 0 && (!d_states_in || !d_states_out || !d_energies))
         return set_err(err, errlen, B200SA_EINVAL, "device buffers are NULL");
@@ -635,6 +579,8 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
     int rc = B200SA_OK;
     if (mode == B200SA_MODE_PERSISTENT) {
         rc = run_persistent(plan, a, st, err, errlen);
+    } else if (mode == B200SA_MODE_GRAPH) {
+        rc = run_graph(plan, a, st, err, errlen);
     } else {
         for (int i = 0; i < plan->num_problems && rc == B200SA_OK; ++i) {
             const int64_t o = plan->plain_item_off[i];

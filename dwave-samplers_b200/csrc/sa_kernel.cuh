@@ -46,10 +46,12 @@ constexpr double kTwo64 = 18446744073709551616.0;  // (double)RANDMAX
 // the host libm's exp (each within ~1 ulp of the true value) could disagree.
 constexpr double kTieRel = 3.552713678800501e-15;  // 2^-48
 
+// Stream positions are kept modulo 2^32: only their differences (all below
+// kRing) and their residues modulo kRing are used, and both survive the wrap.
 struct RingState {
     uint64_t t0, t1;  // this lane's segment-start state for the next refill
-    uint64_t q;       // outputs consumed so far (stream position, warp-uniform)
-    uint64_t base;    // ring holds positions [base, base + kRing)
+    uint32_t q;       // outputs consumed so far (stream position, warp-uniform)
+    uint32_t base;    // ring holds positions [base, base + kRing)
 };
 
 struct Counters {
@@ -139,7 +141,7 @@ struct Prob {
     const double *__restrict__ betas;
     const double *__restrict__ thresholds;
     const uint8_t *__restrict__ dist;
-    const unsigned long long *__restrict__ share;
+    const uint32_t *__restrict__ share;
     int regular_degree;
     uint32_t regular_magic;
 };
@@ -195,10 +197,10 @@ __device__ __forceinline__ void xs_jump(uint64_t &s0, uint64_t &s1) {
 
 // Lane l writes stream positions pos + l*kPerLane + t, t < kPerLane, starting
 // from the state that precedes position pos + l*kPerLane.
-__device__ __forceinline__ void ring_fill(uint64_t *ring, uint64_t pos,
+__device__ __forceinline__ void ring_fill(uint64_t *ring, uint32_t pos,
                                           uint64_t s0, uint64_t s1,
                                           unsigned lane) {
-    const uint64_t start = pos + (uint64_t)lane * kPerLane;
+    const uint32_t start = pos + lane * (uint32_t)kPerLane;
 #pragma unroll
     for (int t = 0; t < kPerLane; ++t)
         ring[(start + t) & (kRing - 1)] = xs_next(s0, s1);
@@ -223,7 +225,7 @@ __device__ __forceinline__ void ring_init(uint64_t *ring, RingState &rs,
 // Overwrites the consumed lower half with the positions kRing further on and
 // returns this lane's next segment-start state.  Out of line: it runs once per
 // kHalf draws.
-__device__ __noinline__ ulonglong2 ring_refill_half(uint64_t *ring, uint64_t pos,
+__device__ __noinline__ ulonglong2 ring_refill_half(uint64_t *ring, uint32_t pos,
                                                     ulonglong2 t, unsigned lane) {
     __syncwarp();
     ring_fill(ring, pos, t.x, t.y, lane);
@@ -237,7 +239,7 @@ __device__ __noinline__ ulonglong2 ring_refill_half(uint64_t *ring, uint64_t pos
 // it is overwritten with the positions kRing further on.
 __device__ __forceinline__ void ring_refill(uint64_t *ring, RingState &rs,
                                             unsigned lane) {
-    if (rs.q - rs.base >= (uint64_t)kHalf) {
+    if (rs.q - rs.base >= (uint32_t)kHalf) {
         const ulonglong2 t =
             ring_refill_half(ring, rs.base + kRing, make_ulonglong2(rs.t0, rs.t1), lane);
         rs.t0 = t.x;
@@ -351,18 +353,18 @@ __device__ __forceinline__ void apply_flips(const Prob &P, double *de, int8_t *s
 }
 
 // Neighbour updates of the committed flips for equal-length lists (D entries
-// each, list v at v * D).  `rank_tab[f]` describes the f-th committed flip in
-// variable order: window position + 256 * (spin before the flip), so the
-// position is its low byte and the spin the arithmetic shift by 8.  The entries of the first 64 accepted flips were loaded
-// into (nb0, w0, k0) / (nb1, w1, k1) before the commit point was known (the
-// committed flips are a prefix of the accepted ones); later entries are
-// loaded here.  Equal targets within a round are summed in entry order by
-// their first lane, as in apply_flips.
+// each, list v at v * D).  `rank_tab[f]` is the lane of the f-th committed
+// flip in variable order; `mult` is each lane's (int8)(4 * s) as a double
+// (cpu_sa.cpp:172), read by the entry's owner lane.  The entries of the first
+// 64 accepted flips were loaded into (nb0, w0, k0) / (nb1, w1, k1) before the
+// commit point was known (the committed flips are a prefix of the accepted
+// ones); later entries are loaded here.  Equal targets within a round are
+// summed in entry order by their first lane, as in apply_flips.
 __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t *sp,
                                                double *scratch, const int *rank_tab,
                                                int nflips, int p, int nb0, double w0, int k0,
                                                int nb1, double w1, int k1, bool may_conflict,
-                                               unsigned lane) {
+                                               double mult, unsigned lane) {
     const int D = P.regular_degree;
     const int total = nflips * D;
     for (int base = 0; base < total; base += 32) {
@@ -379,15 +381,15 @@ __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t
             if (a) {
                 const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
                 k = rank_tab[r];
-                const int e = (p + (k & 0xff)) * D + (t - r * D);
+                const int e = (p + k) * D + (t - r * D);
                 nb = __ldg(&P.col[e]);
                 wt = __ldg(&P.w[e]);
             }
         }
+        const double m_k = __shfl_sync(kFull, mult, k);
         double x = 0.0;
         if (a) {
-            const double mult = (double)(int)(int8_t)(4 * (k >> 8));  // cpu_sa.cpp:172
-            x = __dmul_rn(__dmul_rn(mult, wt), (double)(int)sp[nb]);
+            x = __dmul_rn(__dmul_rn(m_k, wt), (double)(int)sp[nb]);
         } else {
             nb = -1 - (int)lane;  // distinct per inactive lane
         }
@@ -413,14 +415,16 @@ __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t
 }
 
 // Sequential order (cpu_sa.cpp:132-192) in speculative passes over windows
-// of 32*S consecutive variables, S per lane (slot s of lane l is window
-// position 32*s + l).
-template <bool GIBBS, int S>
+// of 32 consecutive variables, one per lane.  Every lane decides its variable
+// against the delta energies at the start of the pass; the pass commits the
+// prefix of the window that ends before the first variable whose decision a
+// committed flip could have changed (a later neighbour of an accepted flip),
+// so the committed decisions equal the sequential ones.
+template <bool GIBBS>
 __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                                                  int8_t *sp, double *scratch,
                                                  uint64_t *ring, RingState &rs,
                                                  unsigned lane, Counters &cnt) {
-    constexpr int W = 32 * S;
     const int n = P.n;
     const int D = P.regular_degree;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -432,81 +436,49 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
             int p = 0;
             while (p < n) {
                 ring_refill(ring, rs, lane);
-                const int L = min(W, n - p);
-                double d[S];
-                int dist[S];
-                unsigned long long shr[S];
-                uint2 vi[S];
-                bool act[S];
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    const int pos = 32 * s + (int)lane;
-                    act[s] = pos < L;
-                    d[s] = 0.0;
-                    dist[s] = (int)kDistCap;
-                    shr[s] = 0ull;
-                    vi[s] = make_uint2(0u, 0u);
-                    if (act[s]) {
-                        d[s] = de[p + pos];
-                        dist[s] = __ldg(&P.dist[p + pos]);
-                        shr[s] = __ldg(&P.share[p + pos]);
-                        if (!D) vi[s] = __ldg(&P.vinfo[p + pos]);
+                const int L = min(32, n - p);
+                const int v = p + (int)lane;
+                const bool act = (int)lane < L;
+                double d = 0.0;
+                int dist = (int)kDistCap;
+                uint32_t shr = 0u;
+                uint2 vi = make_uint2(0u, 0u);
+                if (act) {
+                    d = de[v];
+                    dist = __ldg(&P.dist[v]);
+                    shr = __ldg(&P.share[v]);
+                    if (!D) vi = __ldg(&P.vinfo[v]);
+                }
+                const bool consider = act && !(d >= thr);  // cpu_sa.cpp:140
+                const bool need = GIBBS ? consider : (consider && !(d <= 0.0));
+                const unsigned nm = __ballot_sync(kFull, need);
+                bool acc = GIBBS ? false : consider;  // Metropolis: d <= 0 accepts
+                bool near = false;
+                if (need) {
+                    const uint64_t r = ring[(rs.q + (uint32_t)__popc(nm & lt_mask)) & (kRing - 1)];
+                    const int fast = GIBBS ? gibbs_fast(__dmul_rn(d, beta), r)
+                                           : metropolis_fast(__dmul_rn(-d, beta), r);
+                    if (fast >= 0) {
+                        acc = fast != 0;
+                    } else {
+                        const int ex = GIBBS ? gibbs_exact(d, beta, r) : metropolis_exact(d, beta, r);
+                        acc = (ex & 1) != 0;
+                        near = (ex & 2) != 0;
                     }
                 }
-                unsigned nm[S];
-                bool acc[S], near[S];
-                uint64_t rbase = rs.q;
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    const bool consider = act[s] && !(d[s] >= thr);  // cpu_sa.cpp:140
-                    const bool need = GIBBS ? consider : (consider && !(d[s] <= 0.0));
-                    nm[s] = __ballot_sync(kFull, need);
-                    acc[s] = GIBBS ? false : consider;  // Metropolis: d <= 0 accepts
-                    near[s] = false;
-                    if (need) {
-                        const uint64_t r =
-                            ring[(rbase + (uint64_t)__popc(nm[s] & lt_mask)) & (kRing - 1)];
-                        const int fast = GIBBS ? gibbs_fast(__dmul_rn(d[s], beta), r)
-                                               : metropolis_fast(__dmul_rn(-d[s], beta), r);
-                        if (fast >= 0) {
-                            acc[s] = fast != 0;
-                        } else {
-                            const int ex = GIBBS ? gibbs_exact(d[s], beta, r)
-                                                 : metropolis_exact(d[s], beta, r);
-                            acc[s] = (ex & 1) != 0;
-                            near[s] = (ex & 2) != 0;
-                        }
-                    }
-                    rbase += (uint64_t)__popc(nm[s]);
-                }
-                unsigned am[S];
-                unsigned any_acc = 0u;
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    am[s] = __ballot_sync(kFull, acc[s]);
-                    any_acc |= am[s];
-                }
+                const unsigned am = __ballot_sync(kFull, acc);
                 // Equal-length lists: start loading the accepted flips'
                 // adjacency before the commit point is known.
                 int nb0 = 0, nb1 = 0, k0 = 0, k1 = 0;
                 double w0 = 0.0, w1 = 0.0;
-                if (D && any_acc) {
-                    int abase = 0;
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        if (acc[s]) {
-                            const int pos = 32 * s + (int)lane;
-                            rank_tab[abase + __popc(am[s] & lt_mask)] =
-                                pos + 256 * (int)sp[p + pos];
-                        }
-                        abase += __popc(am[s]);
-                    }
+                if (D && am) {
+                    if (acc) rank_tab[__popc(am & lt_mask)] = (int)lane;
                     __syncwarp();
-                    const int pre = min(abase * D, 64);
+                    const int pre = min(__popc(am) * D, 64);
                     if ((int)lane < pre) {
                         const int r = (int)((lane * P.regular_magic) >> 16);
                         k0 = rank_tab[r];
-                        const int e = (p + (k0 & 0xff)) * D + ((int)lane - r * D);
+                        const int e = (p + k0) * D + ((int)lane - r * D);
                         nb0 = __ldg(&P.col[e]);
                         w0 = __ldg(&P.w[e]);
                     }
@@ -514,61 +486,39 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                         const int t = (int)lane + 32;
                         const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
                         k1 = rank_tab[r];
-                        const int e = (p + (k1 & 0xff)) * D + (t - r * D);
+                        const int e = (p + k1) * D + (t - r * D);
                         nb1 = __ldg(&P.col[e]);
                         w1 = __ldg(&P.w[e]);
                     }
                 }
-                int bound = W;
-#pragma unroll
-                for (int s = 0; s < S; ++s)
-                    if (acc[s]) bound = min(bound, 32 * s + (int)lane + dist[s]);
+                const int bound = acc ? (int)lane + dist : 32;
                 const int c = min(__reduce_min_sync(kFull, bound), L);
-                unsigned fm[S];
-                int nflips = 0;
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    const int cs = c - 32 * s;
-                    const unsigned cm = cs >= 32 ? kFull : (cs <= 0 ? 0u : ((1u << cs) - 1u));
-                    rs.q += (uint64_t)__popc(nm[s] & cm);
-                    fm[s] = am[s] & cm;
-                    cnt.near += __popc(__ballot_sync(kFull, near[s]) & cm);
-                    nflips += __popc(fm[s]);
-                }
-                cnt.flips += nflips;
+                const unsigned commit = c >= 32 ? kFull : ((1u << c) - 1u);
+                rs.q += (uint32_t)__popc(nm & commit);
+                const unsigned fm = am & commit;
+                cnt.near += __popc(__ballot_sync(kFull, near) & commit);
+                cnt.flips += __popc(fm);
                 cnt.passes += 1;
-                if (nflips) {
+                if (fm) {
+                    const int s_cur = act ? (int)sp[v] : 0;
                     // A slot can receive two additions only through a repeated
                     // target in one list or a neighbour common to two flips.
-                    unsigned long long fm64 = fm[0];
-                    if (S > 1) fm64 |= (unsigned long long)fm[S - 1] << 32;
-                    bool risk = false;
-#pragma unroll
-                    for (int s = 0; s < S; ++s) {
-                        const int pos = 32 * s + (int)lane;
-                        if ((fm[s] >> lane) & 1u) {
-                            const unsigned long long later = pos < 63 ? fm64 >> (pos + 1) : 0ull;
-                            risk |= (shr[s] & 1ull) || ((shr[s] >> 1) & later);
-                        }
-                    }
-                    const bool may_conflict = __any_sync(kFull, risk);
+                    const unsigned later = lane < 31 ? fm >> (lane + 1) : 0u;
+                    const bool f = (fm >> lane) & 1u;
+                    const bool may_conflict =
+                        __any_sync(kFull, f && ((shr & 1u) || ((shr >> 1) & later)));
                     if (D) {
-                        update_regular(P, de, sp, scratch, rank_tab, nflips, p, nb0, w0, k0, nb1,
-                                       w1, k1, may_conflict, lane);
-#pragma unroll
-                        for (int s = 0; s < S; ++s) {
-                            if ((fm[s] >> lane) & 1u) {  // cpu_sa.cpp:189-190
-                                const int v = p + 32 * s + (int)lane;
-                                sp[v] = (int8_t)(-(int)sp[v]);
-                                de[v] = __dmul_rn(de[v], -1.0);
-                            }
+                        update_regular(P, de, sp, scratch, rank_tab, __popc(fm), p, nb0, w0, k0,
+                                       nb1, w1, k1, may_conflict,
+                                       (double)(int)(int8_t)(4 * s_cur), lane);
+                        if (f) {  // cpu_sa.cpp:189-190, after the variable's own updates
+                            sp[v] = (int8_t)(-s_cur);
+                            de[v] = __dmul_rn(de[v], -1.0);
                         }
                         __syncwarp();
-                    } else if constexpr (S == 1) {
-                        const int v = p + (int)lane;
-                        const int s_old = act[0] ? (int)sp[v] : 0;
-                        apply_flips(P, de, sp, scratch, fm[0], v, (int)vi[0].x,
-                                    (int)(vi[0].y & kDegMask), s_old, may_conflict, lane);
+                    } else {
+                        apply_flips(P, de, sp, scratch, fm, v, (int)vi.x,
+                                    (int)(vi.y & kDegMask), s_cur, may_conflict, lane);
                     }
                 }
                 p += c;
@@ -657,7 +607,7 @@ __device__ __forceinline__ double state_energy(const ProblemDev *PD, const int8_
     return e;
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, int S>
+template <bool GIBBS, bool RANDOM_ORDER>
 __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *src,
                                             int8_t *dst, double *energy_out,
                                             double *de, int8_t *sp,
@@ -670,7 +620,7 @@ __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *
         if (RANDOM_ORDER)
             sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
         else
-            sweep_sequential<GIBBS, S>(P, de, sp, scratch, ring, rs, lane, cnt);
+            sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
     }
     __syncwarp();
     const double e = state_energy(PD, sp, lane);

@@ -10,7 +10,7 @@
 
 namespace b200sa {
 
-template <bool GIBBS, bool RANDOM_ORDER, bool SMEM, int S>
+template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
 __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
     sa_warp_kernel(LaunchArgs A, int warps_per_cta, int region_bytes) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -39,8 +39,8 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
         for (int i = lane; i < kRing; i += 32) ring[i] = A.rng_carry[i];
         rs.t0 = A.rng_carry[kRing + 2 * lane];
         rs.t1 = A.rng_carry[kRing + 2 * lane + 1];
-        rs.q = A.rng_carry[kRing + kCarryLaneWords];
-        rs.base = A.rng_carry[kRing + kCarryLaneWords + 1];
+        rs.q = (uint32_t)A.rng_carry[kRing + kCarryLaneWords];
+        rs.base = (uint32_t)A.rng_carry[kRing + kCarryLaneWords + 1];
         stream_live = true;
         __syncwarp();
     }
@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
         }
         const int64_t so = PD->state_offset + (int64_t)r * PD->n;
         Counters cnt = {0ull, 0ull, 0u};
-        anneal_read<GIBBS, RANDOM_ORDER, S>(PD, A.states_in + so, A.states_out + so,
+        anneal_read<GIBBS, RANDOM_ORDER>(PD, A.states_in + so, A.states_out + so,
                                             &A.energies[rd], de, sp, scratch, ring, rs, lane,
                                             cnt);
         if (lane == 0) {
@@ -90,21 +90,15 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
 using KernelFn = void (*)(LaunchArgs, int, int);
 
 static KernelFn kernel_for(int variant) {
-    switch (variant & 15) {
-        case 0: return sa_warp_kernel<false, false, false, 1>;
-        case 1: return sa_warp_kernel<true, false, false, 1>;
-        case 2: return sa_warp_kernel<false, true, false, 1>;
-        case 3: return sa_warp_kernel<true, true, false, 1>;
-        case 4: return sa_warp_kernel<false, false, true, 1>;
-        case 5: return sa_warp_kernel<true, false, true, 1>;
-        case 6: return sa_warp_kernel<false, true, true, 1>;
-        case 7: return sa_warp_kernel<true, true, true, 1>;
-        // 64-variable windows (sequential order only)
-        case 8: return sa_warp_kernel<false, false, false, 2>;
-        case 9: return sa_warp_kernel<true, false, false, 2>;
-        case 12: return sa_warp_kernel<false, false, true, 2>;
-        case 13: return sa_warp_kernel<true, false, true, 2>;
-        default: return nullptr;
+    switch (variant & 7) {
+        case 0: return sa_warp_kernel<false, false, false>;
+        case 1: return sa_warp_kernel<true, false, false>;
+        case 2: return sa_warp_kernel<false, true, false>;
+        case 3: return sa_warp_kernel<true, true, false>;
+        case 4: return sa_warp_kernel<false, false, true>;
+        case 5: return sa_warp_kernel<true, false, true>;
+        case 6: return sa_warp_kernel<false, true, true>;
+        default: return sa_warp_kernel<true, true, true>;
     }
 }
 

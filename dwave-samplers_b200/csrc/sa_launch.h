@@ -11,10 +11,9 @@ namespace b200sa {
 constexpr int kMaxThreadsPerCta = 512;
 
 // Kernel variant: bit 0 Gibbs, bit 1 random order, bit 2 state in shared
-// memory, bit 3 64-variable windows (sequential order, equal-length lists).
-inline int kernel_variant(bool gibbs, bool random_order, bool smem, bool wide = false) {
-    return (gibbs ? 1 : 0) | (random_order ? 2 : 0) | (smem ? 4 : 0) |
-           (wide && !random_order ? 8 : 0);
+// memory.
+inline int kernel_variant(bool gibbs, bool random_order, bool smem) {
+    return (gibbs ? 1 : 0) | (random_order ? 2 : 0) | (smem ? 4 : 0);
 }
 
 cudaError_t upload_jump_table(const uint32_t table[][4], cudaStream_t stream);

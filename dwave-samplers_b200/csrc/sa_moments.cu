@@ -152,3 +152,69 @@ extern "C" int b200sa_edge_moments(const b200sa_moments_problem *problems, int32
     if (e != cudaSuccess) return fail(err, errlen, B200SA_ECUDA, cudaGetErrorString(e));
     return (int)tiles.size();
 }
+
+// ---- Counter-based initial states --------------------------------------------
+// Uniform +-1 spins as a hash of (init_seed, model, read, variable): the
+// splitmix64 finalizer applied to a key of (init_seed, model) and then to
+// key ^ (read * 0x100000001B3 + variable); the spin is +1 when the top bit of
+// the result is set.  Any range of reads regenerates identically, which is
+// what lets sampled states be recomputed from seeds instead of stored.
+namespace {
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// Each thread writes 16 consecutive spins of the flattened (reads x n) block.
+__global__ void random_states_kernel(uint64_t key, int64_t read0, int64_t total, int32_t n,
+                                     int8_t *out) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x * 16;
+    for (int64_t base = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 16; base < total;
+         base += stride) {
+        int64_t r = base / n;
+        int32_t i = (int32_t)(base - r * n);
+        const int64_t end = base + 16 < total ? base + 16 : total;
+        for (int64_t k = base; k < end; ++k) {
+            const uint64_t x = mix64(key ^ ((uint64_t)(read0 + r) * 0x100000001B3ull + (uint64_t)i));
+            out[k] = (x >> 63) ? 1 : -1;
+            if (++i == n) {
+                i = 0;
+                ++r;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int b200sa_random_states(uint64_t init_seed, uint64_t model_index, int64_t read0,
+                                    int64_t num_reads, int32_t num_vars, int8_t *d_states,
+                                    int32_t device, void *stream, char *err, size_t errlen) {
+    if (num_reads < 0 || num_vars < 0 || read0 < 0)
+        return fail(err, errlen, B200SA_EINVAL, "negative size");
+    const int64_t total = num_reads * (int64_t)num_vars;
+    if (total == 0) return 0;
+    if (!d_states) return fail(err, errlen, B200SA_EINVAL, "null state buffer");
+    int prev = -1;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(err, errlen, B200SA_ENODEV, cudaGetErrorString(e));
+    const uint64_t key = [&] {
+        uint64_t x = init_seed * 0x9E3779B97F4A7C15ull + model_index * 0xD1B54A32D192ED03ull;
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        return x ^ (x >> 31);
+    }();
+    constexpr int kBlock = 256;
+    const int64_t threads = (total + 15) / 16;
+    int64_t blocks = (threads + kBlock - 1) / kBlock;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    random_states_kernel<<<(unsigned)blocks, kBlock, 0, static_cast<cudaStream_t>(stream)>>>(
+        key, read0, total, num_vars, d_states);
+    e = cudaGetLastError();
+    if (prev >= 0) cudaSetDevice(prev);
+    if (e != cudaSuccess) return fail(err, errlen, B200SA_ECUDA, cudaGetErrorString(e));
+    return 0;
+}

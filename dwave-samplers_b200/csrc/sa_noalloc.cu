@@ -55,7 +55,7 @@ constexpr size_t kOffCursor = align256(kOffProb + sizeof(ProblemDev));  // int[n
 constexpr size_t kOffVinfo = align256(kOffCursor + 4 * kNoAllocMaxVars);
 constexpr size_t kOffDist = align256(kOffVinfo + 8 * kNoAllocMaxVars);
 constexpr size_t kOffShare = align256(kOffDist + kNoAllocMaxVars);
-constexpr size_t kOffCol = align256(kOffShare + 8 * kNoAllocMaxVars);
+constexpr size_t kOffCol = align256(kOffShare + 4 * kNoAllocMaxVars);
 constexpr size_t kOffW = align256(kOffCol + 4 * 2 * kNoAllocMaxCouplers);
 constexpr size_t kOffThr = align256(kOffW + 8 * 2 * kNoAllocMaxCouplers);
 constexpr size_t kOffItems = align256(kOffThr + 8 * kNoAllocMaxBetas);
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
     int *cursor = reinterpret_cast<int *>(a.base + kOffCursor);
     uint2 *vinfo = reinterpret_cast<uint2 *>(a.base + kOffVinfo);
     uint8_t *dist = a.base + kOffDist;
-    unsigned long long *share = reinterpret_cast<unsigned long long *>(a.base + kOffShare);
+    uint32_t *share = reinterpret_cast<uint32_t *>(a.base + kOffShare);
     int32_t *col = reinterpret_cast<int32_t *>(a.base + kOffCol);
     double *w = reinterpret_cast<double *>(a.base + kOffW);
     double *thr = reinterpret_cast<double *>(a.base + kOffThr);
@@ -150,9 +150,8 @@ __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
         }
     }
     __syncthreads();
-    // Per-variable records: degree and nearest later neighbour; conflict
-    // masks set conservatively (all bits) so the sweep always groups equal
-    // targets.
+    // Speculation records: nearest later neighbour; conflict masks set
+    // conservatively (all bits) so the sweep always groups equal targets.
     for (int v = tid; v < a.n; v += nt) {
         const uint2 vi = vinfo[v];
         unsigned dmin = kDistCap;
@@ -160,9 +159,8 @@ __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
             const int u = col[e];
             if (u > v && (unsigned)(u - v) < dmin) dmin = (unsigned)(u - v);
         }
-        vinfo[v] = make_uint2(vi.x, vi.y | (dmin << kDistShift));
         dist[v] = (uint8_t)dmin;
-        share[v] = ~0ull;
+        share[v] = ~0u;
     }
     for (int b = tid; b < a.num_betas; b += nt) thr[b] = 44.36142 / a.betas[b];
     for (int r = tid; r < a.num_reads; r += nt) items[r] = (int64_t)r;  // problem 0, read r

@@ -15,17 +15,23 @@ constexpr int kRing = 256;
 constexpr int kHalf = kRing / 2;
 constexpr int kPerLane = kHalf / 32;
 
-// Per-variable record (uint2), one load per variable and pass:
-//   x          : start of the variable's adjacency list
-//   y bits 0-23: degree (list length)
-//   y bits 24-31: distance to the nearest later neighbour (u - v for the
-//                smallest neighbour u > v), capped at kDistCap.  A flip of v
-//                can only change the decision of a variable inside the
-//                current window if that variable is at least this far ahead.
+// Per-variable adjacency record (uint2): x = start of the variable's list,
+// y = its degree (list length).
 constexpr uint32_t kDegMask = 0x00ffffffu;
-constexpr int kDistShift = 24;
-constexpr uint32_t kDistCap = 64;  // the widest speculative window
 constexpr uint32_t kMaxDegree = kDegMask;
+
+// Speculation arrays, read once per variable and pass (kept as two compact
+// arrays, 5 bytes per variable, so they stay in the L1 left beside the
+// shared regions):
+//   dist:  distance to the nearest later neighbour (u - v for the smallest
+//          neighbour u > v), capped at kDistCap.  A flip of v can only change
+//          the decision of a later variable of the current window if that
+//          variable is at least this far ahead.
+//   share: conflict mask.  Bit 0 is set when v's list names a target twice;
+//          bit j (1..31) when v and v + j have a common neighbour.  Two
+//          committed flips can add into the same delta-energy slot only
+//          through one of these.
+constexpr uint32_t kDistCap = 32;  // the speculative window
 
 struct ProblemDev {
     int32_t n;
@@ -35,12 +41,9 @@ struct ProblemDev {
     int64_t m;              // couplers
     int64_t state_offset;   // element offset of read 0 in the state arrays
     int64_t read_offset;    // offset of read 0 in energies / seeds / stats
-    const uint2 *vinfo;     // [n] per-variable record (see above)
-    const uint8_t *dist;    // [n] the record's distance field alone (compact, L1-resident)
-    // [n] conflict mask: bit 0 set when v's list names a target twice; bit j
-    // (1..63) set when v and v + j have a common neighbour.  Two committed
-    // flips can add into the same slot only through one of these.
-    const unsigned long long *share;
+    const uint2 *vinfo;     // [n] adjacency record (see above)
+    const uint8_t *dist;    // [n] speculation distance (see above)
+    const uint32_t *share;  // [n] conflict mask (see above)
     const int32_t *col;     // [2m] neighbour index, coupler input order
     const double *w;        // [2m] coupling
     const double *h;        // [n]
@@ -95,9 +98,9 @@ constexpr int kCarryLaneWords = 64;                 // 32 lanes x 2 words
 constexpr int kCarryWords = kRing + kCarryLaneWords + 2;  // ring, lanes, q, base
 
 // Per-warp shared region: RNG ring, scratch (32 doubles for equal-slot sums,
-// 64 ints for the rank table of accepted flips), delta energies, spins.
+// 32 ints for the rank table of accepted flips), delta energies, spins.
 // (region_bytes_for keeps every region a multiple of 16 bytes.)
-constexpr int kScratchBytes = 32 * 8 + 64 * 4;
+constexpr int kScratchBytes = 32 * 8 + 32 * 4;
 inline int region_bytes_for(int cap_n) {
     const int spins = (cap_n + 15) & ~15;
     return kRing * 8 + kScratchBytes + cap_n * 8 + spins;

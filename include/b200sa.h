@@ -57,6 +57,8 @@ extern "C" {
 /* Scheduling modes for the batched entry points. */
 #define B200SA_MODE_PERSISTENT 0 /* one launch, device work queue over (problem, read) */
 #define B200SA_MODE_PLAIN 1      /* one launch per problem, problems in order */
+#define B200SA_MODE_GRAPH 2      /* the persistent launches captured once as a CUDA graph
+                                    (plans only; replayed while the buffers are the same) */
 
 /* Replaces the reference's `callback` (cpu_sa.h:61): called between reads,
  * in read order, for each completed read; nonzero stops sampling and the
@@ -138,13 +140,51 @@ B200SA_API int b200sa_plan_layout(b200sa_plan plan, int64_t *state_offsets,
  * cudaStream_t; NULL selects the plan's own stream (pass cudaStreamLegacy for
  * the legacy default stream).  The call returns after the
  * work is enqueued when `sync` is 0, and after it completes when 1 (stats
- * are filled only when sync is 1). */
+ * are filled only when sync is 1).  Runs of one plan must not overlap in time
+ * (they share the plan's queue heads, counters and global slots). */
 B200SA_API int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
                     int8_t *d_states_out, double *d_energies,
                     const uint64_t *d_seeds, void *stream, int32_t sync,
                     b200sa_stats *stats, char *err, size_t errlen);
 
 B200SA_API int b200sa_plan_destroy(b200sa_plan plan);
+
+/* Replaces the fields h[num_vars] and coupler weights J[num_couplers] (host
+ * arrays, COO order as at creation) of problem `problem`; couplers, schedule
+ * and seeds are kept, and so is a captured graph.  Waits for the plan's last
+ * run and returns when the device copy is updated.  No reference counterpart:
+ * for learning loops that re-sample the same models with new parameters. */
+B200SA_API int b200sa_plan_set_weights(b200sa_plan plan, int32_t problem, const double *h,
+                                       const double *J, char *err, size_t errlen);
+
+/* ---- Autotuner (no reference counterpart) ---------------------------------
+ * For every non-empty bucket of a plan (size class x acceptance rule x order)
+ * times candidate launch configurations -- warps per CTA, CTAs per SM, and
+ * delta energies / spins in shared memory or in a global slot -- on a sample
+ * of the bucket's reads (its largest problems, 16 betas spread over each
+ * schedule) and keeps the fastest for the plan's persistent and graph runs.
+ * Every configuration computes the same results; only speed changes.  The
+ * choices are cached in the text file `cache_path` (NULL: no file), keyed by
+ * GPU, library version, kind, size and mean degree, and reused unless flags
+ * has B200SA_TUNE_FORCE.  Writes up to report_cap entries and returns the
+ * number of non-empty buckets, or a negative error. */
+#define B200SA_TUNE_FORCE 1
+typedef struct {
+    int32_t bucket;
+    int32_t kind;           /* bit 0 Gibbs, bit 1 random order */
+    int32_t max_n;
+    int64_t items;          /* reads in the bucket */
+    int32_t onchip;         /* 1: state in shared memory */
+    int32_t warps_per_cta;
+    int32_t ctas_per_sm;
+    double attempts_per_s;  /* measured on the sample */
+    int32_t from_cache;
+    int32_t candidates;     /* configurations measured (0 when cached) */
+} b200sa_tune_entry;
+
+B200SA_API int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags,
+                                    b200sa_tune_entry *report, int32_t report_cap, char *err,
+                                    size_t errlen);
 
 /* ---- Sample moments (no reference counterpart) ------------------------------
  * For the gradient of log Z of p(s) ~ exp(-beta*E(s)), E as in cpu_sa.cpp:210-227:
@@ -166,6 +206,17 @@ typedef struct {
 
 B200SA_API int b200sa_edge_moments(const b200sa_moments_problem *problems, int32_t num_problems,
                                    int32_t device, void *stream, char *err, size_t errlen);
+
+/* No counterpart in the reference.  Writes num_reads x num_vars uniform +-1
+ * initial states (reads read0 .. read0+num_reads-1 of model model_index) to
+ * device memory as a counter-based hash of (init_seed, model, read, variable),
+ * so that any range of reads can be regenerated identically (samples are
+ * recomputed from their seeds instead of stored).  Asynchronous on `stream`
+ * (a cudaStream_t; NULL = legacy default stream).  Returns 0 or a negative
+ * error. */
+B200SA_API int b200sa_random_states(uint64_t init_seed, uint64_t model_index, int64_t read0,
+                                    int64_t num_reads, int32_t num_vars, int8_t *d_states,
+                                    int32_t device, void *stream, char *err, size_t errlen);
 
 /* No counterpart in the reference.  The sampler for callers that cannot
  * allocate device memory while they run (all device memory owned by a

@@ -146,3 +146,14 @@ def test_batched_boltzmann_machine_learning_reduces_correlation_error():
                  target_sweeps=300, seed=3)
     assert res.corr_error[-1] < 0.5 * res.corr_error[0], res.corr_error[::8]
     assert res.steps_per_second > 0
+
+
+@pytest.mark.parametrize("init_seed, model, read0, reads, n", [
+    (8, 0, 0, 256, 16), (1, 3, 77, 5, 1), (2**40 + 5, 63, 1000, 33, 17), (0, 0, 0, 300, 2048)])
+def test_device_initial_states_match_host(init_seed, model, read0, reads, n):
+    from b200sa.autograd import device_initial_states
+    out = torch.empty(reads * n, dtype=torch.int8, device="cuda")
+    device_initial_states(out, init_seed, model, read0, reads, n)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy().reshape(reads, n),
+                                  initial_states(init_seed, model, reads, n, read0))

@@ -1,0 +1,135 @@
+"""Plan features with no reference counterpart, checked against the plan's
+own persistent runs and the oracle: CUDA-graph replay, in-place weight
+updates, and the autotuner (its choices must not change any result)."""
+import copy
+
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from b200sa import Plan, workloads
+from b200sa.workloads import Instance, random_regular, random_states
+from conftest import bits
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_batch(seed=31):
+    """Small uneven problems plus one above the on-chip size (global state)."""
+    probs = workloads.uneven_batch(num_problems=10, n_range=(64, 900), reads_range=(3, 24),
+                                   sweeps_range=(10, 60), seed=seed)
+    rng = np.random.default_rng(seed)
+    n, u, v = random_regular(9000, 4, rng, graph_seed=seed)
+    probs.append(Instance(rng.normal(0, 0.1, n), u, v, rng.normal(0, 1, u.shape[0]),
+                          random_states(rng, 5, n), np.geomspace(0.1, 5.0, 8), 1,
+                          np.arange(5, dtype=np.uint64) + 99))
+    k16 = workloads.complete_graph(reads=16, sweeps=30, seed=seed)
+    probs.append(k16)  # Gibbs
+    return probs
+
+
+def device_buffers(plan, probs):
+    host = np.concatenate([p.states.ravel() for p in probs])
+    sin = torch.from_numpy(host).cuda()
+    out = torch.empty_like(sin)
+    en = torch.empty(plan.total_reads, dtype=torch.float64, device="cuda")
+    return sin, out, en
+
+
+def test_graph_replay_equals_persistent():
+    probs = mixed_batch()
+    with Plan(probs) as plan:
+        sin, ref, en_ref = device_buffers(plan, probs)
+        plan.run(sin, ref, en_ref, mode="persistent")
+        out = torch.empty_like(ref)
+        en = torch.empty_like(en_ref)
+        for _ in range(3):  # capture, then two replays
+            out.zero_()
+            st = plan.run(sin, out, en, mode="graph")
+            assert torch.equal(out, ref) and torch.equal(en, en_ref)
+            assert st["attempts"] == plan.attempts and st["launches"] >= 1
+        out2 = torch.empty_like(ref)  # new buffers: captured again
+        plan.run(sin, out2, en, mode="graph")
+        assert torch.equal(out2, ref)
+
+
+def test_set_weights_equals_fresh_plan():
+    probs = mixed_batch(seed=37)[:6]
+    rng = np.random.default_rng(5)
+    new = copy.deepcopy(probs)
+    for k in (1, 4):
+        new[k].h = rng.normal(0, 0.3, new[k].n)
+        new[k].J = rng.normal(0, 1.0, new[k].J.shape[0])
+    with Plan(probs) as plan, Plan(new) as fresh:
+        sin, out, en = device_buffers(plan, probs)
+        plan.run(sin, out, en, mode="graph")  # a captured graph survives the update
+        for k in (1, 4):
+            plan.set_weights(k, new[k].h, new[k].J)
+        plan.run(sin, out, en, mode="graph")
+        _, out_f, en_f = device_buffers(fresh, new)
+        fresh.run(sin, out_f, en_f)
+        assert torch.equal(out, out_f) and torch.equal(en, en_f)
+        p = new[1]
+        ws, we = oracle.run(p.h, p.u, p.v, p.J, p.states, p.sweeps_per_beta, p.betas, p.seeds)
+        o = int(plan.state_offsets[1])
+        got = out[o:o + p.num_reads * p.n].cpu().numpy().reshape(p.num_reads, p.n)
+        np.testing.assert_array_equal(got, ws)
+        r = int(plan.read_offsets[1])
+        np.testing.assert_array_equal(bits(en[r:r + p.num_reads].cpu().numpy()), bits(we))
+    with Plan(probs) as plan:
+        with pytest.raises(ValueError):
+            plan.set_weights(len(probs), probs[0].h, probs[0].J)
+
+
+def test_autotune_keeps_results_and_caches(tmp_path):
+    probs = mixed_batch(seed=41)
+    cache = str(tmp_path / "tune.txt")
+    with Plan(probs) as plan:
+        sin, ref, en_ref = device_buffers(plan, probs)
+        plan.run(sin, ref, en_ref)
+        rep = plan.autotune(cache, force=True)
+        assert rep and all(e["candidates"] >= 1 and e["from_cache"] == 0 for e in rep)
+        assert all(e["warps_per_cta"] >= 1 and e["attempts_per_s"] > 0 for e in rep)
+        assert sum(e["items"] for e in rep) == plan.total_reads
+        out = torch.empty_like(ref)
+        en = torch.empty_like(en_ref)
+        for mode in ("persistent", "graph"):
+            out.zero_()
+            plan.run(sin, out, en, mode=mode)
+            assert torch.equal(out, ref) and torch.equal(en, en_ref)
+    lines = open(cache).read().splitlines()
+    assert len(lines) >= 1 and all(len(x.split()) == 5 for x in lines)
+    with Plan(probs) as plan:
+        rep2 = plan.autotune(cache)
+        assert all(e["from_cache"] == 1 and e["candidates"] == 0 for e in rep2)
+        sin, out, en = device_buffers(plan, probs)
+        plan.run(sin, out, en)
+        assert torch.equal(out, ref)
+
+
+def test_concurrent_global_buckets_do_not_share_slots():
+    """Two problems above the on-chip size with different kernels run as two
+    concurrent bucket launches; each must use its own global slots."""
+    rng = np.random.default_rng(43)
+    probs = []
+    for k, crit in enumerate(("Metropolis", "Gibbs", "Metropolis")):
+        n, u, v = random_regular(9000, 3 + k, rng, graph_seed=50 + k)
+        probs.append(Instance(rng.normal(0, 0.1, n), u, v, rng.normal(0, 1, u.shape[0]),
+                              random_states(rng, 6, n), np.geomspace(0.1, 5.0, 6), 1,
+                              np.arange(6, dtype=np.uint64) + 7 * k, proposal=crit,
+                              randomize_order=(k == 2)))
+    with Plan(probs) as plan:
+        sin, a, ea = device_buffers(plan, probs)
+        plan.run(sin, a, ea, mode="persistent")
+        b = torch.empty_like(a)
+        eb = torch.empty_like(ea)
+        plan.run(sin, b, eb, mode="plain")
+        assert torch.equal(a, b) and torch.equal(ea, eb)
+        for k in (0, 1):
+            p = probs[k]
+            ws, we = oracle.run(p.h, p.u, p.v, p.J, p.states, 1, p.betas, p.seeds,
+                                False, p.proposal == "Gibbs")
+            o = int(plan.state_offsets[k])
+            got = a[o:o + p.num_reads * p.n].cpu().numpy().reshape(p.num_reads, p.n)
+            np.testing.assert_array_equal(got, ws)
