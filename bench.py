@@ -55,6 +55,11 @@ def parse_args():
                     help="scale every schedule's length (profiling captures only; "
                          "1.0 is the benchmark workload)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (occupancy rule per bucket)")
+    ap.add_argument("--mode", choices=["graph", "persistent"], default="graph",
+                    help="batched runs: persistent launches replayed as a CUDA graph, or issued "
+                         "one by one")
     ap.add_argument("--bm-steps", type=int, default=2,
                     help="timed Boltzmann-machine gradient steps (after one untimed step)")
     ap.add_argument("--bm-target-reads", type=int, default=1024,
@@ -362,6 +367,16 @@ def run_ours(args):
     probs = workload(args, rank)
     attempts = int(sum(p.attempts for p in probs))
     plan = Plan(probs, device=local)
+    tune = None
+    if not args.no_tune:
+        import tempfile
+        cache = os.path.join(tempfile.gettempdir(), f"b200sa_tune_{os.getpid()}.txt")
+        t0 = time.perf_counter()
+        entries = plan.autotune(cache, force=True)
+        tune = {"seconds": time.perf_counter() - t0, "buckets": [
+            {k: e[k] for k in ("max_n", "items", "onchip", "warps_per_cta", "ctas_per_sm",
+                               "candidates")} for e in entries]}
+        os.environ["B200SA_TUNE_CACHE"] = cache  # the e2e call reuses these choices
     host_states = np.concatenate([p.states.ravel() for p in probs])
     sin = torch.from_numpy(host_states).cuda()
     sout = torch.empty_like(sin)
@@ -390,13 +405,15 @@ def run_ours(args):
         return e0.elapsed_time(e1)
 
     with Clocks(local) as clk:
-        total_ms = timed("persistent", args.warmup, args.steps)
+        total_ms = timed(args.mode, args.warmup, args.steps)
     total_ms = max_over_ranks(total_ms, world, "cuda")
     ms_step = total_ms / args.steps
     value = world * attempts / (ms_step / 1000.0)
 
     # Counters of the last warm-up run (deterministic for these inputs).
-    stats = run_stats["persistent"]
+    if args.mode not in run_stats:
+        run_stats[args.mode] = plan.run(sin, sout, en, mode=args.mode, stream=stream, sync=True)
+    stats = run_stats[args.mode]
     flips = stats["flips"]
     if stats["attempts"] != attempts:
         raise RuntimeError(f"attempt count mismatch: {stats['attempts']} != {attempts}")
@@ -405,7 +422,11 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": workload_config(args, probs) | {"parallelism": f"independent batch per GPU x{world}"},
+        "config": workload_config(args, probs) | {
+            "parallelism": f"independent batch per GPU x{world}",
+            "batched_runs": ("persistent launches replayed as one CUDA graph" if args.mode == "graph"
+                             else "persistent launches"),
+            "autotune": tune},
     }
     peak, peak_src = measured_hbm_peak()
     abytes = algorithmic_bytes(probs, flips)
@@ -437,7 +458,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         t0 = time.perf_counter()
-        sample_batch(work, mode="persistent", device=local)
+        sample_batch(work, mode=args.mode, device=local)
         dt = time.perf_counter() - t0
         e2e_times.append(max_over_ranks(dt, world, "cuda"))
     if e2e_times:

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -625,6 +626,11 @@ int b200sa_sample_batch(const b200sa_problem *problems, int32_t num_problems, in
     int rc = b200sa_plan_create(problems, num_problems, device, &plan, err, errlen);
     if (rc) return rc;
     std::unique_ptr<b200sa_plan_s, int (*)(b200sa_plan)> hold(plan, b200sa_plan_destroy);
+    const char *cache = std::getenv("B200SA_TUNE_CACHE");
+    if (cache && *cache && mode != B200SA_MODE_PLAIN) {
+        rc = b200sa_plan_autotune(plan, cache, 0, nullptr, 0, err, errlen);
+        if (rc < 0) return rc;
+    }
     DeviceGuard guard;
     B200SA_CUDA(cudaSetDevice(plan->device));
     DevArray<int8_t> dstates;

@@ -112,7 +112,10 @@ B200SA_API int b200sa_sample(int32_t num_vars, const double *h, int64_t num_coup
 
 /* Many independent problems (uneven sizes, read counts and schedules), host
  * buffers.  The reference has no batched entry point; each problem's reads
- * equal the per-read reference calls.  mode: B200SA_MODE_*.
+ * equal the per-read reference calls.  mode: B200SA_MODE_*.  When the
+ * environment variable B200SA_TUNE_CACHE names a file, persistent and graph
+ * runs use the autotuner's choices from it (measuring buckets it lacks; see
+ * b200sa_plan_autotune).
  * Returns the total number of reads completed or a negative error. */
 B200SA_API int b200sa_sample_batch(const b200sa_problem *problems, int32_t num_problems,
                         int32_t mode, int32_t device, b200sa_stats *stats,
