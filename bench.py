@@ -375,7 +375,7 @@ def run_ours(args):
         entries = plan.autotune(cache, force=True)
         tune = {"seconds": time.perf_counter() - t0, "buckets": [
             {k: e[k] for k in ("max_n", "items", "onchip", "warps_per_cta", "ctas_per_sm",
-                               "candidates")} for e in entries]}
+                               "registers", "candidates")} for e in entries]}
         os.environ["B200SA_TUNE_CACHE"] = cache  # the e2e call reuses these choices
     host_states = np.concatenate([p.states.ravel() for p in probs])
     sin = torch.from_numpy(host_states).cuda()

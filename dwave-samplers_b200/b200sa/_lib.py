@@ -103,6 +103,7 @@ class TuneEntry(ctypes.Structure):
         ("onchip", ctypes.c_int32),
         ("warps_per_cta", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32),
+        ("registers", ctypes.c_int32),
         ("attempts_per_s", ctypes.c_double),
         ("from_cache", ctypes.c_int32),
         ("candidates", ctypes.c_int32),

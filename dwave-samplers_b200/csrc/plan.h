@@ -104,6 +104,7 @@ struct TuneChoice {
     bool onchip = true;     // delta energies and spins in shared memory (if they fit)
     int warps_per_cta = 0;
     int ctas_per_sm = 0;    // 0: as many as fit
+    int reg_class = 0;      // kernel register budget: 0 = 128, 1 = 80, 2 = 64 per thread
     double rate = 0.0;      // measured attempts/s of the choice
 };
 

@@ -62,7 +62,8 @@ namespace {
 
 // ---- autotuner ---------------------------------------------------------------
 
-constexpr int kTuneBetas = 16;  // betas per sampled schedule
+constexpr int kTuneBetas = 8;     // betas per sampled schedule
+constexpr int kTuneWarpsPerSm = 64;  // sample reads per SM: two waves at 32 warps per SM
 
 std::string tune_key(const b200sa_plan_s *P, int kind, int max_n, int mean_degree) {
     std::string name = P->prop.name;
@@ -78,7 +79,7 @@ std::string tune_key(const b200sa_plan_s *P, int kind, int max_n, int mean_degre
     return s;
 }
 
-// Cache lines: "<key> <onchip> <warps_per_cta> <ctas_per_sm> <attempts/s>".
+// Cache lines: "<key> <onchip> <warps_per_cta> <ctas_per_sm> <reg_class> <attempts/s>".
 std::map<std::string, TuneChoice> load_cache(const char *path) {
     std::map<std::string, TuneChoice> out;
     if (!path) return out;
@@ -87,15 +88,17 @@ std::map<std::string, TuneChoice> load_cache(const char *path) {
     while (std::getline(f, line)) {
         std::istringstream in(line);
         std::string key;
-        int onchip = 0, w = 0, ctas = 0;
+        int onchip = 0, w = 0, ctas = 0, regs = 0;
         double rate = 0.0;
-        if (!(in >> key >> onchip >> w >> ctas >> rate)) continue;
-        if (w < 1 || w > kMaxThreadsPerCta / 32 || ctas < 0) continue;
+        if (!(in >> key >> onchip >> w >> ctas >> regs >> rate)) continue;
+        if (w < 1 || w > kMaxThreadsPerCta / 32 || ctas < 0 || regs < 0 || regs >= kRegClasses)
+            continue;
         TuneChoice c;
         c.set = true;
         c.onchip = onchip != 0;
         c.warps_per_cta = w;
         c.ctas_per_sm = ctas;
+        c.reg_class = regs;
         c.rate = rate;
         out[key] = c;
     }
@@ -110,7 +113,8 @@ bool save_cache(const char *path, const std::map<std::string, TuneChoice> &cache
         if (!f) return false;
         for (const auto &kv : cache)
             f << kv.first << ' ' << (kv.second.onchip ? 1 : 0) << ' ' << kv.second.warps_per_cta
-              << ' ' << kv.second.ctas_per_sm << ' ' << kv.second.rate << '\n';
+              << ' ' << kv.second.ctas_per_sm << ' ' << kv.second.reg_class << ' '
+              << kv.second.rate << '\n';
         if (!f) return false;
     }
     return std::rename(tmp.c_str(), path) == 0;
@@ -330,7 +334,7 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
         const int max_n = plan->bucket_max_n[b];
         TuneSample S;
         int mean_degree = 0;
-        int rc = build_sample(plan, b, (int64_t)sms * (kMaxThreadsPerCta / 32), S, &mean_degree,
+        int rc = build_sample(plan, b, (int64_t)sms * kTuneWarpsPerSm, S, &mean_degree,
                               err, errlen);
         if (rc) return rc;
         const std::string key = tune_key(plan, kind, max_n, mean_degree);
@@ -342,15 +346,16 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
             best = hit->second;
             cached = true;
         } else {
-            // Candidates: per staging, every warps-per-CTA whose resident
-            // warps per SM come within 3/4 of that staging's best, at full
-            // occupancy and with one CTA fewer per SM (more L1 beside the
-            // shared regions).
+            // Candidates: per register budget and staging, every
+            // warps-per-CTA whose resident warps per SM come within 7/8 of
+            // that pair's best, at full occupancy, plus the largest such CTA
+            // with one CTA fewer per SM (more L1 beside the shared regions).
             std::vector<TuneChoice> cands;
+            for (int regs = 0; regs < kRegClasses; ++regs)
             for (int onchip = 1; onchip >= 0; --onchip) {
                 if (onchip && max_n > plan->onchip_max) continue;
                 const int region = region_bytes_for(onchip ? max_n : 0);
-                const int variant = kernel_variant(kind & 1, kind & 2, onchip != 0);
+                const int variant = kernel_variant(kind & 1, kind & 2, onchip != 0, regs);
                 int resident[kMaxThreadsPerCta / 32 + 1] = {};
                 int ctas_of[kMaxThreadsPerCta / 32 + 1] = {};
                 int top = 0;
@@ -361,16 +366,21 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
                     resident[w] = ctas_of[w] * w;
                     top = std::max(top, resident[w]);
                 }
+                int widest = 0;
                 for (int w = 1; w <= kMaxThreadsPerCta / 32; ++w) {
-                    if (resident[w] == 0 || 4 * resident[w] < 3 * top) continue;
-                    for (int limit = 0; limit <= (ctas_of[w] > 1 ? 1 : 0); ++limit) {
-                        TuneChoice c;
-                        c.set = true;
-                        c.onchip = onchip != 0;
-                        c.warps_per_cta = w;
-                        c.ctas_per_sm = limit ? ctas_of[w] - 1 : 0;
-                        cands.push_back(c);
-                    }
+                    if (resident[w] == 0 || 8 * resident[w] < 7 * top) continue;
+                    TuneChoice c;
+                    c.set = true;
+                    c.onchip = onchip != 0;
+                    c.warps_per_cta = w;
+                    c.reg_class = regs;
+                    cands.push_back(c);
+                    widest = w;
+                }
+                if (widest && ctas_of[widest] > 1) {
+                    TuneChoice c = cands.back();
+                    c.ctas_per_sm = ctas_of[widest] - 1;
+                    cands.push_back(c);
                 }
             }
             float best_ms = 0.f;
@@ -400,6 +410,7 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
             e.onchip = best.onchip && max_n <= plan->onchip_max ? 1 : 0;
             e.warps_per_cta = best.warps_per_cta;
             e.ctas_per_sm = best.ctas_per_sm;
+            e.registers = best.reg_class == 1 ? kRegs80 : best.reg_class == 2 ? kRegs64 : 128;
             e.attempts_per_s = best.rate;
             e.from_cache = cached ? 1 : 0;
             e.candidates = measured;

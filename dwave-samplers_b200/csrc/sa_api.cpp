@@ -83,7 +83,8 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
     const bool onchip = choice && choice->set ? choice->onchip : true;
     const int cap = onchip && max_n_here <= P->onchip_max ? max_n_here : 0;
     const int region = region_bytes_for(cap);
-    const int variant = kernel_variant(kind & 1, kind & 2, cap > 0);
+    const int reg_class = choice && choice->set && persistent ? choice->reg_class : 0;
+    const int variant = kernel_variant(kind & 1, kind & 2, cap > 0, reg_class);
     if (choice && choice->set && persistent) {
         // The autotuner's measured configuration.
         const int w = choice->warps_per_cta;

@@ -2,7 +2,10 @@
 // device work-queue head (persistent mode: one launch per bucket) or by a
 // static stride (plain mode: one launch per problem).  One instantiation per
 // acceptance rule, update order and state location, so each keeps only its
-// own path's registers.
+// own path's registers, and per register budget: 128 registers a thread (at
+// most 16 warps per SM), 80 (24 warps) or 64 (32 warps).  Fewer registers
+// mean more spills but more reads in flight per SM, which pays when a bucket
+// has enough reads to fill them; the autotuner chooses per bucket.
 #include <cuda_runtime.h>
 
 #include "sa_kernel.cuh"
@@ -11,8 +14,8 @@
 namespace b200sa {
 
 template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
-__global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
-    sa_warp_kernel(LaunchArgs A, int warps_per_cta, int region_bytes) {
+__device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_cta,
+                                             int region_bytes) {
     extern __shared__ __align__(16) uint8_t smem[];
     const unsigned lane = threadIdx.x & 31u;
     const int wid = (int)(threadIdx.x >> 5);
@@ -87,18 +90,40 @@ __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
     }
 }
 
+template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
+__global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
+    sa_warp_kernel(LaunchArgs A, int warps_per_cta, int region_bytes) {
+    sa_warp_body<GIBBS, RANDOM_ORDER, SMEM>(A, warps_per_cta, region_bytes);
+}
+
+template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
+__global__ void __maxnreg__(kRegs80) sa_warp_kernel_r80(LaunchArgs A, int warps_per_cta,
+                                                         int region_bytes) {
+    sa_warp_body<GIBBS, RANDOM_ORDER, SMEM>(A, warps_per_cta, region_bytes);
+}
+
+template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
+__global__ void __maxnreg__(kRegs64) sa_warp_kernel_r64(LaunchArgs A, int warps_per_cta,
+                                                         int region_bytes) {
+    sa_warp_body<GIBBS, RANDOM_ORDER, SMEM>(A, warps_per_cta, region_bytes);
+}
+
 using KernelFn = void (*)(LaunchArgs, int, int);
 
+#define B200SA_KERNEL_TABLE(name)                                                       \
+    {name<false, false, false>, name<true, false, false>, name<false, true, false>,    \
+     name<true, true, false>,   name<false, false, true>, name<true, false, true>,     \
+     name<false, true, true>,   name<true, true, true>}
+
 static KernelFn kernel_for(int variant) {
-    switch (variant & 7) {
-        case 0: return sa_warp_kernel<false, false, false>;
-        case 1: return sa_warp_kernel<true, false, false>;
-        case 2: return sa_warp_kernel<false, true, false>;
-        case 3: return sa_warp_kernel<true, true, false>;
-        case 4: return sa_warp_kernel<false, false, true>;
-        case 5: return sa_warp_kernel<true, false, true>;
-        case 6: return sa_warp_kernel<false, true, true>;
-        default: return sa_warp_kernel<true, true, true>;
+    static const KernelFn k128[8] = B200SA_KERNEL_TABLE(sa_warp_kernel);
+    static const KernelFn k80[8] = B200SA_KERNEL_TABLE(sa_warp_kernel_r80);
+    static const KernelFn k64[8] = B200SA_KERNEL_TABLE(sa_warp_kernel_r64);
+    switch (variant >> 3) {
+        case 0: return k128[variant & 7];
+        case 1: return k80[variant & 7];
+        case 2: return k64[variant & 7];
+        default: return nullptr;
     }
 }
 

@@ -9,11 +9,16 @@
 namespace b200sa {
 
 constexpr int kMaxThreadsPerCta = 512;
+// Register budgets of the sweep kernels (per thread): 128 (launch bounds of
+// 512 threads, one CTA), kRegs80 and kRegs64.
+constexpr int kRegs80 = 80;
+constexpr int kRegs64 = 64;
+constexpr int kRegClasses = 3;  // 0: 128, 1: 80, 2: 64
 
 // Kernel variant: bit 0 Gibbs, bit 1 random order, bit 2 state in shared
-// memory.
-inline int kernel_variant(bool gibbs, bool random_order, bool smem) {
-    return (gibbs ? 1 : 0) | (random_order ? 2 : 0) | (smem ? 4 : 0);
+// memory, bits 3-4 register class (0: 128, 1: 80, 2: 64 registers).
+inline int kernel_variant(bool gibbs, bool random_order, bool smem, int reg_class = 0) {
+    return (gibbs ? 1 : 0) | (random_order ? 2 : 0) | (smem ? 4 : 0) | (reg_class << 3);
 }
 
 cudaError_t upload_jump_table(const uint32_t table[][4], cudaStream_t stream);

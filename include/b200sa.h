@@ -162,9 +162,11 @@ B200SA_API int b200sa_plan_set_weights(b200sa_plan plan, int32_t problem, const 
 
 /* ---- Autotuner (no reference counterpart) ---------------------------------
  * For every non-empty bucket of a plan (size class x acceptance rule x order)
- * times candidate launch configurations -- warps per CTA, CTAs per SM, and
- * delta energies / spins in shared memory or in a global slot -- on a sample
- * of the bucket's reads (its largest problems, 16 betas spread over each
+ * times candidate launch configurations -- warps per CTA, CTAs per SM, the
+ * kernel's register budget (128, 80 or 64 registers a thread: fewer spill
+ * more but let more reads run per SM), and delta energies / spins in shared
+ * memory or in a global slot -- on a sample
+ * of the bucket's reads (its largest problems, 8 betas spread over each
  * schedule) and keeps the fastest for the plan's persistent and graph runs.
  * Every configuration computes the same results; only speed changes.  The
  * choices are cached in the text file `cache_path` (NULL: no file), keyed by
@@ -180,6 +182,7 @@ typedef struct {
     int32_t onchip;         /* 1: state in shared memory */
     int32_t warps_per_cta;
     int32_t ctas_per_sm;
+    int32_t registers;      /* register budget per thread of the chosen kernel */
     double attempts_per_s;  /* measured on the sample */
     int32_t from_cache;
     int32_t candidates;     /* configurations measured (0 when cached) */

@@ -91,6 +91,7 @@ def test_autotune_keeps_results_and_caches(tmp_path):
         rep = plan.autotune(cache, force=True)
         assert rep and all(e["candidates"] >= 1 and e["from_cache"] == 0 for e in rep)
         assert all(e["warps_per_cta"] >= 1 and e["attempts_per_s"] > 0 for e in rep)
+        assert all(e["registers"] in (64, 80, 128) for e in rep)
         assert sum(e["items"] for e in rep) == plan.total_reads
         out = torch.empty_like(ref)
         en = torch.empty_like(en_ref)
@@ -99,7 +100,7 @@ def test_autotune_keeps_results_and_caches(tmp_path):
             plan.run(sin, out, en, mode=mode)
             assert torch.equal(out, ref) and torch.equal(en, en_ref)
     lines = open(cache).read().splitlines()
-    assert len(lines) >= 1 and all(len(x.split()) == 5 for x in lines)
+    assert len(lines) >= 1 and all(len(x.split()) == 6 for x in lines)
     with Plan(probs) as plan:
         rep2 = plan.autotune(cache)
         assert all(e["from_cache"] == 1 and e["candidates"] == 0 for e in rep2)
@@ -133,3 +134,37 @@ def test_concurrent_global_buckets_do_not_share_slots():
             o = int(plan.state_offsets[k])
             got = a[o:o + p.num_reads * p.n].cpu().numpy().reshape(p.num_reads, p.n)
             np.testing.assert_array_equal(got, ws)
+
+
+def test_batch_with_other_spin_values_matches_oracle():
+    """Initial spins other than +-1 (the reference's int8 arithmetic is
+    defined for them) mixed with ordinary reads in one batch, in every mode,
+    against the oracle."""
+    rng = np.random.default_rng(47)
+    probs = []
+    for k, crit in enumerate(("Metropolis", "Gibbs")):
+        n, u, v = random_regular(300 + 50 * k, 5, rng, graph_seed=60 + k)
+        st = random_states(rng, 10, n)
+        st[1, 7] = 2
+        st[4, :5] = [0, -3, 5, 127, -128]
+        probs.append(Instance(rng.normal(0, 0.1, n), u, v, rng.normal(0, 1, u.shape[0]), st,
+                              np.geomspace(0.1, 3.0, 20), 2, np.arange(10, dtype=np.uint64) + 3,
+                              proposal=crit))
+    with Plan(probs) as plan:
+        sin, ref, en_ref = device_buffers(plan, probs)
+        plan.run(sin, ref, en_ref, mode="persistent")
+        for k, p in enumerate(probs):
+            ws, we = oracle.run(p.h, p.u, p.v, p.J, p.states, p.sweeps_per_beta, p.betas,
+                                p.seeds, False, p.proposal == "Gibbs")
+            o = int(plan.state_offsets[k])
+            got = ref[o:o + p.num_reads * p.n].cpu().numpy().reshape(p.num_reads, p.n)
+            np.testing.assert_array_equal(got, ws)
+            r = int(plan.read_offsets[k])
+            np.testing.assert_array_equal(bits(en_ref[r:r + p.num_reads].cpu().numpy()),
+                                          bits(we))
+        for mode in ("plain", "graph"):
+            out = torch.empty_like(ref)
+            en = torch.empty_like(en_ref)
+            st = plan.run(sin, out, en, mode=mode)
+            assert torch.equal(out, ref) and torch.equal(en, en_ref), mode
+            assert st["reads"] == plan.total_reads
