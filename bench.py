@@ -37,6 +37,10 @@ from b200sa import workloads  # noqa: E402
 METRIC = "spin-flip attempts/s, 1 B200: batched vs plain (bit-exact); BM grad steps/s"
 UNIT = "attempts/s"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) of one step's sweep launches on the full batch with
+# autotuned launches, from an ncu capture (metrics dram__bytes_read.sum and
+# dram__bytes_write.sum, one pass per launch): profiles/uneven_batch_step_dram_traffic.md.
+TRAFFIC_BYTES_PER_STEP = 2.473e13
 
 
 def parse_args():
@@ -55,6 +59,10 @@ def parse_args():
                     help="scale every schedule's length (profiling captures only; "
                          "1.0 is the benchmark workload)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--n-range", type=int, nargs=2, default=None,
+                    help="problem sizes (profiling captures only; default 64 4096)")
+    ap.add_argument("--reads-range", type=int, nargs=2, default=None,
+                    help="reads per problem (profiling captures only; default 32 1024)")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (occupancy rule per bucket)")
     ap.add_argument("--mode", choices=["graph", "persistent"], default="graph",
@@ -78,8 +86,18 @@ def max_over_ranks(x: float, world: int, device=None) -> float:
     return float(t.item())
 
 
+def full_workload(args) -> bool:
+    return (args.problems == 512 and args.sweep_scale == 1.0 and not args.n_range
+            and not args.reads_range)
+
+
 def workload(args, rank=0):
-    probs = workloads.uneven_batch(num_problems=args.problems)
+    kw = {}
+    if args.n_range:
+        kw["n_range"] = tuple(args.n_range)
+    if args.reads_range:
+        kw["reads_range"] = tuple(args.reads_range)
+    probs = workloads.uneven_batch(num_problems=args.problems, **kw)
     if args.sweep_scale != 1.0:
         for p in probs:
             k = max(1, int(round(len(p.betas) * args.sweep_scale)))
@@ -432,7 +450,8 @@ def run_ours(args):
     abytes = algorithmic_bytes(probs, flips)
     achieved = abytes / (ms_step / 1000.0) / 1e9
     line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak, "traffic": None,
+                        "frac": achieved / peak,
+                        "traffic": (TRAFFIC_BYTES_PER_STEP if full_workload(args) else None),
                         "peak_source": peak_src,
                         "algorithmic_bytes_per_launch": abytes}
     line["clocks"] = clk.summary()
