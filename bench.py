@@ -87,15 +87,15 @@ def max_over_ranks(x: float, world: int, device=None) -> float:
 
 
 def full_workload(args) -> bool:
-    return (args.problems == 512 and args.sweep_scale == 1.0 and not args.n_range
-            and not args.reads_range)
+    return (args.problems == 512 and args.sweep_scale == 1.0
+            and not getattr(args, "n_range", None) and not getattr(args, "reads_range", None))
 
 
 def workload(args, rank=0):
     kw = {}
-    if args.n_range:
+    if getattr(args, "n_range", None):
         kw["n_range"] = tuple(args.n_range)
-    if args.reads_range:
+    if getattr(args, "reads_range", None):
         kw["reads_range"] = tuple(args.reads_range)
     probs = workloads.uneven_batch(num_problems=args.problems, **kw)
     if args.sweep_scale != 1.0:
@@ -392,7 +392,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         entries = plan.autotune(cache, force=True)
         tune = {"seconds": time.perf_counter() - t0, "buckets": [
-            {k: e[k] for k in ("max_n", "items", "onchip", "warps_per_cta", "ctas_per_sm",
+            {k: e[k] for k in ("max_n", "items", "staging", "warps_per_cta", "ctas_per_sm",
                                "registers", "candidates")} for e in entries]}
         os.environ["B200SA_TUNE_CACHE"] = cache  # the e2e call reuses these choices
     host_states = np.concatenate([p.states.ravel() for p in probs])

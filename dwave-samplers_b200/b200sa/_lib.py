@@ -100,7 +100,7 @@ class TuneEntry(ctypes.Structure):
         ("kind", ctypes.c_int32),
         ("max_n", ctypes.c_int32),
         ("items", ctypes.c_int64),
-        ("onchip", ctypes.c_int32),
+        ("staging", ctypes.c_int32),
         ("warps_per_cta", ctypes.c_int32),
         ("ctas_per_sm", ctypes.c_int32),
         ("registers", ctypes.c_int32),

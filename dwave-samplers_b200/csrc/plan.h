@@ -101,7 +101,7 @@ inline int kind_of(const ProblemDev &d) {
 // occupancy rule of shape_for).
 struct TuneChoice {
     bool set = false;
-    bool onchip = true;     // delta energies and spins in shared memory (if they fit)
+    int staging = kStageShared;  // state location (kStage*), used where it fits
     int warps_per_cta = 0;
     int ctas_per_sm = 0;    // 0: as many as fit
     int reg_class = 0;      // kernel register budget: 0 = 128, 1 = 80, 2 = 64 per thread
@@ -109,7 +109,8 @@ struct TuneChoice {
 };
 
 struct LaunchShape {
-    int cap_n;         // largest n kept in shared memory
+    int stage;         // state location (kStage*)
+    int cap_n;         // largest n whose shared-memory part fits the region
     int warps_per_cta;
     int region;
     int grid;

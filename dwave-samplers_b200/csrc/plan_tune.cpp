@@ -79,7 +79,7 @@ std::string tune_key(const b200sa_plan_s *P, int kind, int max_n, int mean_degre
     return s;
 }
 
-// Cache lines: "<key> <onchip> <warps_per_cta> <ctas_per_sm> <reg_class> <attempts/s>".
+// Cache lines: "<key> <staging> <warps_per_cta> <ctas_per_sm> <reg_class> <attempts/s>".
 std::map<std::string, TuneChoice> load_cache(const char *path) {
     std::map<std::string, TuneChoice> out;
     if (!path) return out;
@@ -88,14 +88,15 @@ std::map<std::string, TuneChoice> load_cache(const char *path) {
     while (std::getline(f, line)) {
         std::istringstream in(line);
         std::string key;
-        int onchip = 0, w = 0, ctas = 0, regs = 0;
+        int staging = 0, w = 0, ctas = 0, regs = 0;
         double rate = 0.0;
-        if (!(in >> key >> onchip >> w >> ctas >> regs >> rate)) continue;
-        if (w < 1 || w > kMaxThreadsPerCta / 32 || ctas < 0 || regs < 0 || regs >= kRegClasses)
+        if (!(in >> key >> staging >> w >> ctas >> regs >> rate)) continue;
+        if (w < 1 || w > kMaxThreadsPerCta / 32 || ctas < 0 || regs < 0 || regs >= kRegClasses ||
+            staging < kStageGlobal || staging > kStageSpins)
             continue;
         TuneChoice c;
         c.set = true;
-        c.onchip = onchip != 0;
+        c.staging = staging;
         c.warps_per_cta = w;
         c.ctas_per_sm = ctas;
         c.reg_class = regs;
@@ -112,7 +113,7 @@ bool save_cache(const char *path, const std::map<std::string, TuneChoice> &cache
         std::ofstream f(tmp, std::ios::trunc);
         if (!f) return false;
         for (const auto &kv : cache)
-            f << kv.first << ' ' << (kv.second.onchip ? 1 : 0) << ' ' << kv.second.warps_per_cta
+            f << kv.first << ' ' << kv.second.staging << ' ' << kv.second.warps_per_cta
               << ' ' << kv.second.ctas_per_sm << ' ' << kv.second.reg_class << ' '
               << kv.second.rate << '\n';
         if (!f) return false;
@@ -231,7 +232,7 @@ int time_candidate(b200sa_plan_s *P, int kind, int max_n, const TuneChoice &c, T
     LaunchShape s{};
     int rc = shape_for(P, kind, max_n, S.count, true, s, err, errlen, &c);
     if (rc) return rc;
-    if (max_n > s.cap_n) {
+    if (s.stage != kStageShared) {
         rc = ensure_scratch(P, (int64_t)s.grid * s.warps_per_cta, max_n, err, errlen);
         if (rc) return rc;
     }
@@ -352,10 +353,11 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
             // with one CTA fewer per SM (more L1 beside the shared regions).
             std::vector<TuneChoice> cands;
             for (int regs = 0; regs < kRegClasses; ++regs)
-            for (int onchip = 1; onchip >= 0; --onchip) {
-                if (onchip && max_n > plan->onchip_max) continue;
-                const int region = region_bytes_for(onchip ? max_n : 0);
-                const int variant = kernel_variant(kind & 1, kind & 2, onchip != 0, regs);
+            for (int stage : {kStageShared, kStageSpins, kStageGlobal}) {
+                if (stage == kStageShared && max_n > plan->onchip_max) continue;
+                const int region = region_bytes_for_stage(stage, stage == kStageGlobal ? 0 : max_n);
+                if (region > smem_blk) continue;
+                const int variant = kernel_variant(kind & 1, kind & 2, stage, regs);
                 int resident[kMaxThreadsPerCta / 32 + 1] = {};
                 int ctas_of[kMaxThreadsPerCta / 32 + 1] = {};
                 int top = 0;
@@ -371,7 +373,7 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
                     if (resident[w] == 0 || 8 * resident[w] < 7 * top) continue;
                     TuneChoice c;
                     c.set = true;
-                    c.onchip = onchip != 0;
+                    c.staging = stage;
                     c.warps_per_cta = w;
                     c.reg_class = regs;
                     cands.push_back(c);
@@ -407,7 +409,7 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
             e.kind = kind;
             e.max_n = max_n;
             e.items = cnt;
-            e.onchip = best.onchip && max_n <= plan->onchip_max ? 1 : 0;
+            e.staging = best.staging;
             e.warps_per_cta = best.warps_per_cta;
             e.ctas_per_sm = best.ctas_per_sm;
             e.registers = best.reg_class == 1 ? kRegs80 : best.reg_class == 2 ? kRegs64 : 128;

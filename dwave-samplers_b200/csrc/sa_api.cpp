@@ -74,17 +74,22 @@ int occupancy(b200sa_plan_s *P, int variant, int w, int region, int *ctas, char 
 }
 
 // Every warp anneals one read at a time; its shared region holds the RNG
-// ring, the conflict scratch and, when n <= cap_n, the read's delta energies
-// and spins (else those live in a global slot, L2-resident).  Warps per CTA
-// are chosen to maximize resident warps per SM.
+// ring, the conflict scratch and, by the state location, the read's delta
+// energies and spins, its spins only, or neither (the rest lives in a global
+// slot, L2-resident).  Untuned, state is in shared memory whenever it fits
+// and warps per CTA maximize resident warps per SM.
 int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, bool persistent,
               LaunchShape &out, char *err, size_t errlen, const TuneChoice *choice) {
     const int smem_blk = (int)P->prop.sharedMemPerBlockOptin;
-    const bool onchip = choice && choice->set ? choice->onchip : true;
-    const int cap = onchip && max_n_here <= P->onchip_max ? max_n_here : 0;
-    const int region = region_bytes_for(cap);
+    int stage = choice && choice->set ? choice->staging : kStageShared;
+    if (stage == kStageShared && max_n_here > P->onchip_max) stage = kStageGlobal;
+    if (stage == kStageSpins && region_bytes_for_stage(kStageSpins, max_n_here) > smem_blk)
+        stage = kStageGlobal;
+    const int cap = stage == kStageGlobal ? 0 : max_n_here;
+    const int region = region_bytes_for_stage(stage, cap);
     const int reg_class = choice && choice->set && persistent ? choice->reg_class : 0;
-    const int variant = kernel_variant(kind & 1, kind & 2, cap > 0, reg_class);
+    const int variant = kernel_variant(kind & 1, kind & 2, stage, reg_class);
+    out.stage = stage;
     if (choice && choice->set && persistent) {
         // The autotuner's measured configuration.
         const int w = choice->warps_per_cta;
@@ -191,7 +196,7 @@ int launch_shape(b200sa_plan_s *P, LaunchArgs a, const LaunchShape &s, const int
                  unsigned long long *qhead, int64_t slot0, cudaStream_t st, char *err,
                  size_t errlen) {
     if (count <= 0) return B200SA_OK;
-    if (max_n_here > s.cap_n) {
+    if (s.stage != kStageShared) {
         const int64_t end = slot0 + (int64_t)s.grid * s.warps_per_cta;
         if (end > P->scratch_slots || max_n_here > P->scratch_stride)
             return set_err(err, errlen, B200SA_EINVAL, "internal: global slots not reserved");
@@ -218,7 +223,7 @@ int launch_items(b200sa_plan_s *P, LaunchArgs a, int kind, const int64_t *items,
     int rc = items_shape(P, kind, max_n_here, count, persistent, shared_stream, choice, s, err,
                          errlen);
     if (rc) return rc;
-    if (max_n_here > s.cap_n) {
+    if (s.stage != kStageShared) {
         rc = ensure_scratch(P, (int64_t)s.grid * s.warps_per_cta, max_n_here, err, errlen);
         if (rc) return rc;
     }
@@ -267,7 +272,7 @@ int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
         int rc = items_shape(P, b % kKinds, P->bucket_max_n[b], cnt, true, false, &P->tune[b],
                              shape[b], err, errlen);
         if (rc) return rc;
-        if (P->bucket_max_n[b] > shape[b].cap_n) {
+        if (shape[b].stage != kStageShared) {
             slot0[b] = slots;
             slots += (int64_t)shape[b].grid * shape[b].warps_per_cta;
             stride = std::max(stride, P->bucket_max_n[b]);

@@ -13,7 +13,7 @@
 
 namespace b200sa {
 
-template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
+template <bool GIBBS, bool RANDOM_ORDER, int STAGE>
 __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_cta,
                                              int region_bytes) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -26,10 +26,13 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
     const int64_t total_warps = (int64_t)gridDim.x * warps_per_cta;
     double *de;
     int8_t *sp;
-    if (SMEM) {
-        de = reinterpret_cast<double *>(region + kRing * sizeof(uint64_t) + kScratchBytes);
-        sp = reinterpret_cast<int8_t *>(region + kRing * sizeof(uint64_t) + kScratchBytes +
-                                        (size_t)A.smem_cap_n * sizeof(double));
+    uint8_t *state = region + kRing * sizeof(uint64_t) + kScratchBytes;
+    if constexpr (STAGE == kStageShared) {
+        de = reinterpret_cast<double *>(state);
+        sp = reinterpret_cast<int8_t *>(state + (size_t)A.smem_cap_n * sizeof(double));
+    } else if constexpr (STAGE == kStageSpins) {
+        de = A.scratch_de + gw * A.scratch_stride;
+        sp = reinterpret_cast<int8_t *>(state);
     } else {
         de = A.scratch_de + gw * A.scratch_stride;
         sp = A.scratch_s + gw * A.scratch_stride;
@@ -90,39 +93,43 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
     }
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
+template <bool GIBBS, bool RANDOM_ORDER, int STAGE>
 __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
     sa_warp_kernel(LaunchArgs A, int warps_per_cta, int region_bytes) {
-    sa_warp_body<GIBBS, RANDOM_ORDER, SMEM>(A, warps_per_cta, region_bytes);
+    sa_warp_body<GIBBS, RANDOM_ORDER, STAGE>(A, warps_per_cta, region_bytes);
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
+template <bool GIBBS, bool RANDOM_ORDER, int STAGE>
 __global__ void __maxnreg__(kRegs80) sa_warp_kernel_r80(LaunchArgs A, int warps_per_cta,
                                                          int region_bytes) {
-    sa_warp_body<GIBBS, RANDOM_ORDER, SMEM>(A, warps_per_cta, region_bytes);
+    sa_warp_body<GIBBS, RANDOM_ORDER, STAGE>(A, warps_per_cta, region_bytes);
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, bool SMEM>
+template <bool GIBBS, bool RANDOM_ORDER, int STAGE>
 __global__ void __maxnreg__(kRegs64) sa_warp_kernel_r64(LaunchArgs A, int warps_per_cta,
                                                          int region_bytes) {
-    sa_warp_body<GIBBS, RANDOM_ORDER, SMEM>(A, warps_per_cta, region_bytes);
+    sa_warp_body<GIBBS, RANDOM_ORDER, STAGE>(A, warps_per_cta, region_bytes);
 }
 
 using KernelFn = void (*)(LaunchArgs, int, int);
 
-#define B200SA_KERNEL_TABLE(name)                                                       \
-    {name<false, false, false>, name<true, false, false>, name<false, true, false>,    \
-     name<true, true, false>,   name<false, false, true>, name<true, false, true>,     \
-     name<false, true, true>,   name<true, true, true>}
+#define B200SA_KINDS(name, stage)                                                     \
+    name<false, false, stage>, name<true, false, stage>, name<false, true, stage>,   \
+        name<true, true, stage>
+#define B200SA_KERNEL_TABLE(name)                                                     \
+    {B200SA_KINDS(name, kStageGlobal), B200SA_KINDS(name, kStageShared),             \
+     B200SA_KINDS(name, kStageSpins)}
 
 static KernelFn kernel_for(int variant) {
-    static const KernelFn k128[8] = B200SA_KERNEL_TABLE(sa_warp_kernel);
-    static const KernelFn k80[8] = B200SA_KERNEL_TABLE(sa_warp_kernel_r80);
-    static const KernelFn k64[8] = B200SA_KERNEL_TABLE(sa_warp_kernel_r64);
-    switch (variant >> 3) {
-        case 0: return k128[variant & 7];
-        case 1: return k80[variant & 7];
-        case 2: return k64[variant & 7];
+    static const KernelFn k128[12] = B200SA_KERNEL_TABLE(sa_warp_kernel);
+    static const KernelFn k80[12] = B200SA_KERNEL_TABLE(sa_warp_kernel_r80);
+    static const KernelFn k64[12] = B200SA_KERNEL_TABLE(sa_warp_kernel_r64);
+    const int idx = variant & 15;  // kind (bits 0-1) and state location (bits 2-3)
+    if (idx >= 12) return nullptr;
+    switch (variant >> 4) {
+        case 0: return k128[idx];
+        case 1: return k80[idx];
+        case 2: return k64[idx];
         default: return nullptr;
     }
 }

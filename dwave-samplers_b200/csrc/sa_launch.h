@@ -15,10 +15,11 @@ constexpr int kRegs80 = 80;
 constexpr int kRegs64 = 64;
 constexpr int kRegClasses = 3;  // 0: 128, 1: 80, 2: 64
 
-// Kernel variant: bit 0 Gibbs, bit 1 random order, bit 2 state in shared
-// memory, bits 3-4 register class (0: 128, 1: 80, 2: 64 registers).
-inline int kernel_variant(bool gibbs, bool random_order, bool smem, int reg_class = 0) {
-    return (gibbs ? 1 : 0) | (random_order ? 2 : 0) | (smem ? 4 : 0) | (reg_class << 3);
+// Kernel variant: bit 0 Gibbs, bit 1 random order, bits 2-3 state location
+// (kStageGlobal, kStageShared, kStageSpins), bits 4-5 register class (0: 128,
+// 1: 80, 2: 64 registers).
+inline int kernel_variant(bool gibbs, bool random_order, int stage, int reg_class = 0) {
+    return (gibbs ? 1 : 0) | (random_order ? 2 : 0) | (stage << 2) | (reg_class << 4);
 }
 
 cudaError_t upload_jump_table(const uint32_t table[][4], cudaStream_t stream);

@@ -106,4 +106,18 @@ inline int region_bytes_for(int cap_n) {
     return kRing * 8 + kScratchBytes + cap_n * 8 + spins;
 }
 
+// Where a read's state lives: kStageGlobal keeps delta energies and spins in
+// a per-warp global slot (L2-resident), kStageShared both in the warp's
+// shared region, kStageSpins the spins in the shared region and the delta
+// energies in the global slot (a smaller global footprint, and the spin
+// reads of the neighbour updates stay on chip).
+constexpr int kStageGlobal = 0;
+constexpr int kStageShared = 1;
+constexpr int kStageSpins = 2;
+inline int region_bytes_for_stage(int stage, int cap_n) {
+    if (stage == kStageShared) return region_bytes_for(cap_n);
+    if (stage == kStageSpins) return kRing * 8 + kScratchBytes + ((cap_n + 15) & ~15);
+    return kRing * 8 + kScratchBytes;
+}
+
 }  // namespace b200sa

@@ -164,8 +164,9 @@ B200SA_API int b200sa_plan_set_weights(b200sa_plan plan, int32_t problem, const 
  * For every non-empty bucket of a plan (size class x acceptance rule x order)
  * times candidate launch configurations -- warps per CTA, CTAs per SM, the
  * kernel's register budget (128, 80 or 64 registers a thread: fewer spill
- * more but let more reads run per SM), and delta energies / spins in shared
- * memory or in a global slot -- on a sample
+ * more but let more reads run per SM), and where delta energies and spins live
+ * (shared memory, a global slot, or spins shared and energies global) -- on a
+ * sample
  * of the bucket's reads (its largest problems, 8 betas spread over each
  * schedule) and keeps the fastest for the plan's persistent and graph runs.
  * Every configuration computes the same results; only speed changes.  The
@@ -179,7 +180,8 @@ typedef struct {
     int32_t kind;           /* bit 0 Gibbs, bit 1 random order */
     int32_t max_n;
     int64_t items;          /* reads in the bucket */
-    int32_t onchip;         /* 1: state in shared memory */
+    int32_t staging;        /* state: 0 global slot (L2), 1 shared memory, 2 spins in
+                               shared memory and delta energies in the global slot */
     int32_t warps_per_cta;
     int32_t ctas_per_sm;
     int32_t registers;      /* register budget per thread of the chosen kernel */

@@ -168,3 +168,29 @@ def test_batch_with_other_spin_values_matches_oracle():
             st = plan.run(sin, out, en, mode=mode)
             assert torch.equal(out, ref) and torch.equal(en, en_ref), mode
             assert st["reads"] == plan.total_reads
+
+
+def test_every_configuration_gives_identical_results(tmp_path):
+    """Each state location (global slot, shared memory, spins shared with
+    energies global) and register budget, forced through the tuning cache,
+    reproduces the untuned run byte for byte."""
+    probs = workloads.uneven_batch(num_problems=6, n_range=(100, 2500), reads_range=(20, 60),
+                                   sweeps_range=(10, 40), seed=53)
+    probs.append(workloads.complete_graph(reads=40, sweeps=20, seed=53))  # Gibbs
+    cache = tmp_path / "tune.txt"
+    with Plan(probs) as plan:
+        sin, ref, en_ref = device_buffers(plan, probs)
+        plan.run(sin, ref, en_ref)
+        plan.autotune(str(cache), force=True)
+    keys = [line.split()[0] for line in cache.read_text().splitlines()]
+    assert keys
+    for staging in (0, 1, 2):
+        for regs in (0, 1, 2):
+            cache.write_text("".join(f"{k} {staging} 1 0 {regs} 1.0\n" for k in keys))
+            with Plan(probs) as plan:
+                rep = plan.autotune(str(cache))
+                assert all(e["from_cache"] == 1 for e in rep)
+                out = torch.empty_like(ref)
+                en = torch.empty_like(en_ref)
+                plan.run(sin, out, en)
+                assert torch.equal(out, ref) and torch.equal(en, en_ref), (staging, regs)
