@@ -40,7 +40,7 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (read + write) of one step's sweep launches on the full batch with
 # autotuned launches, from an ncu capture (metrics dram__bytes_read.sum and
 # dram__bytes_write.sum, one pass per launch): profiles/uneven_batch_step_dram_traffic.md.
-TRAFFIC_BYTES_PER_STEP = 2.473e13
+TRAFFIC_BYTES_PER_STEP = 2.019e13
 
 
 def parse_args():
