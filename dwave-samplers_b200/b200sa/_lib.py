@@ -43,6 +43,7 @@ EXPORTS = (
     "b200sa_random_states",
     "b200sa_plan_set_weights",
     "b200sa_plan_autotune",
+    "b200sa_steepest_descent",
 )
 
 
@@ -170,6 +171,11 @@ def load() -> ctypes.CDLL:
     L.b200sa_plan_autotune.restype = c.c_int
     L.b200sa_plan_autotune.argtypes = [c.c_void_p, c.c_char_p, c.c_int32, c.POINTER(TuneEntry),
                                        c.c_int32, c.c_char_p, c.c_size_t]
+    L.b200sa_steepest_descent.restype = c.c_int
+    L.b200sa_steepest_descent.argtypes = [
+        c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32,
+        c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32, c.c_uint32, c.c_int32, c.c_char_p,
+        c.c_size_t]
     L.b200sa_version.restype = c.c_char_p
     L.b200sa_version.argtypes = []
     _lib = L

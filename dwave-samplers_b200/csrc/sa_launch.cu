@@ -10,6 +10,7 @@
 
 #include "sa_kernel.cuh"
 #include "sa_launch.h"
+#include "sd_kernel.cuh"
 
 namespace b200sa {
 
@@ -217,6 +218,32 @@ cudaError_t kernel_occupancy(int variant, int warps_per_cta, int region_bytes, i
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k, warps_per_cta * 32, smem);
+}
+
+using SdKernel = void (*)(SdArgs, int, int);
+
+static SdKernel sd_kernel_for(bool sparse, bool smem) {
+    if (sparse) return smem ? sd_warp_kernel<true, true> : sd_warp_kernel<true, false>;
+    return smem ? sd_warp_kernel<false, true> : sd_warp_kernel<false, false>;
+}
+
+cudaError_t launch_sd(bool sparse, bool smem, const SdArgs &args, int grid, int warps_per_cta,
+                      int region_bytes, cudaStream_t stream) {
+    const SdKernel k = sd_kernel_for(sparse, smem);
+    const size_t bytes = (size_t)warps_per_cta * (size_t)region_bytes;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    k<<<grid, warps_per_cta * 32, bytes, stream>>>(args, warps_per_cta, region_bytes);
+    return cudaGetLastError();
+}
+
+cudaError_t sd_occupancy(bool sparse, bool smem, int warps_per_cta, int region_bytes,
+                         int *ctas_per_sm) {
+    const SdKernel k = sd_kernel_for(sparse, smem);
+    const size_t bytes = (size_t)warps_per_cta * (size_t)region_bytes;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k, warps_per_cta * 32, bytes);
 }
 
 }  // namespace b200sa

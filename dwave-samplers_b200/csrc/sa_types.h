@@ -88,6 +88,32 @@ struct LaunchArgs {
     int64_t num_slots;
 };
 
+// Arguments of the steepest-descent kernel (sd_kernel.cuh): one problem,
+// items (0 << 32) | sample taken from a queue head.
+struct SdArgs {
+    const ProblemDev *problem;
+    const int64_t *items;        // (0 << 32) | sample
+    int64_t num_items;
+    unsigned long long *queue_head;
+    const int8_t *states_in;
+    int8_t *states_out;
+    double *energies;
+    uint32_t *steps;
+    uint32_t max_steps;
+    int32_t smem_cap_n;          // state in shared memory when > 0
+    double *scratch_fe;          // else per-warp global slots
+    int8_t *scratch_s;
+    int64_t scratch_stride;
+    unsigned long long *capped;  // samples stopped by max_steps
+};
+
+// Per-warp shared region of the descent kernel: 32 doubles for equal-target
+// sums, then (state in shared memory) flip energies and spins.
+constexpr int kSdScratchBytes = 32 * 8;  // equal-target sums
+inline int sd_region_bytes(int cap_n) {
+    return kSdScratchBytes + cap_n * 8 + ((cap_n + 15) & ~15);
+}
+
 // Nibble tables of the RNG jump matrix: entry [k][v] is the jump applied to
 // the state whose only set bits are the nibble value v at nibble position k.
 constexpr int kJumpNibbles = 32;

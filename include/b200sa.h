@@ -194,6 +194,28 @@ B200SA_API int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, in
                                     b200sa_tune_entry *report, int32_t report_cap, char *err,
                                     size_t errlen);
 
+/* ---- Steepest descent ---------------------------------------------------------
+ * Replaces steepest_gradient_descent (dwave/samplers/greedy/src/descent.cpp:
+ * 315-405, descent.h; bound by dwave/samplers/greedy/descent.pyx:22-112): every
+ * sample descends from its row of `states` (host, num_samples x num_vars int8,
+ * overwritten) by flipping the variable with the most negative flip energy
+ * (ties to the lower index) until none is negative; energies[r] and
+ * num_steps[r] receive its energy and number of flips.  large_sparse_opt
+ * selects the update order of the reference's ordered-set solver (same
+ * selection; neighbours updated with the spin before the flip).  A sample
+ * stops after max_steps flips (0: 1000 * num_vars + 10^6): a self-loop of
+ * positive weight, or spins other than +-1, can make descent cycle (the
+ * reference then never returns); the call then returns B200SA_ETIMEOUT with
+ * the states reached and num_steps == max_steps for those samples.  Returns
+ * num_samples or a negative error. */
+B200SA_API int b200sa_steepest_descent(int32_t num_vars, const double *h, int64_t num_couplers,
+                                       const int32_t *coupler_starts,
+                                       const int32_t *coupler_ends,
+                                       const double *coupler_weights, int32_t num_samples,
+                                       int8_t *states, double *energies, uint32_t *num_steps,
+                                       int32_t large_sparse_opt, uint32_t max_steps,
+                                       int32_t device, char *err, size_t errlen);
+
 /* ---- Sample moments (no reference counterpart) ------------------------------
  * For the gradient of log Z of p(s) ~ exp(-beta*E(s)), E as in cpu_sa.cpp:210-227:
  * d log Z/d h_i = -beta <s_i>, d log Z/d J_c = -beta <s_u(c) s_v(c)>.  Adds the

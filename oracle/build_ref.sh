@@ -1,6 +1,7 @@
 #!/usr/bin/env bash
-# Build the reference's own simulated-annealing extension from its sources, for
-# use as a test oracle and as the timed CPU baseline.  Test infrastructure only.
+# Build the reference's own simulated-annealing and steepest-descent
+# extensions from their sources, for use as test oracles and as the timed CPU
+# baseline.  Test infrastructure only.
 #
 # Sources (read in place, never copied into the repository):
 #   <ref>/dwave/samplers/sa/simulated_annealing.pyx   (Cython binding)
@@ -39,3 +40,18 @@ g++ -O3 -std=c++17 -g1 -DNDEBUG -fPIC -shared -Wall -Wno-unused-function \
 
 rm -f "$OUT/simulated_annealing.cpp"
 echo "built $OUT/simulated_annealing$EXT_SUFFIX"
+
+# The reference's steepest-descent extension (the step after annealing):
+#   <ref>/dwave/samplers/greedy/descent.pyx, decl.pxd   (Cython binding)
+#   <ref>/dwave/samplers/greedy/src/descent.cpp, descent.h (C++ core)
+GR="$REF/dwave/samplers/greedy"
+if [ -f "$GR/descent.pyx" ]; then
+    $PY -m cython --cplus -3 -Xfreethreading_compatible=True -I "$REF" \
+        -o "$OUT/descent.cpp" "$GR/descent.pyx"
+    g++ -O3 -std=c++17 -g1 -DNDEBUG -fPIC -shared -Wall -Wno-unused-function \
+        -I"$GR/src" -I"$PYINC" -I"$NPINC" \
+        "$OUT/descent.cpp" "$GR/src/descent.cpp" \
+        -o "$OUT/descent$EXT_SUFFIX"
+    rm -f "$OUT/descent.cpp"
+    echo "built $OUT/descent$EXT_SUFFIX"
+fi

@@ -11,6 +11,10 @@ Two oracles are exposed:
 * :func:`reference_module` -- the reference's own Cython extension
   (``dwave/samplers/sa/simulated_annealing.pyx``) built from its sources by
   ``oracle/build_ref.sh`` into ``oracle/_ref/``, when that build exists.
+* :func:`descent` -- the C restatement of the reference's steepest descent
+  (``dwave/samplers/greedy/src/descent.cpp:315-405``), and
+  :func:`reference_descent_module`, the reference's own ``descent`` extension
+  built the same way.
 """
 from __future__ import annotations
 
@@ -54,6 +58,11 @@ def lib() -> ctypes.CDLL:
         L.sa_oracle_energy.argtypes = [
             ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.sd_oracle_run.restype = ctypes.c_int
+        L.sd_oracle_run.argtypes = [
+            ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
         L.sa_oracle_rng_stream.restype = None
         L.sa_oracle_rng_stream.argtypes = [ctypes.c_uint64, ctypes.c_int,
                                            ctypes.c_void_p]
@@ -108,6 +117,44 @@ def rng_stream(seed: int, count: int) -> np.ndarray:
     out = np.zeros(count, dtype=np.uint64)
     lib().sa_oracle_rng_stream(int(seed), int(count), _ptr(out))
     return out
+
+
+def descent(h, u, v, J, states, large_sparse_opt=False):
+    """Steepest descent from every row of ``states`` (copied) with the C
+    restatement.  Returns (states, energies, steps)."""
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.int32)
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    st = np.array(states, dtype=np.int8, order="C", copy=True)
+    R = st.shape[0]
+    en = np.zeros(R, dtype=np.float64)
+    steps = np.zeros(R, dtype=np.uint32)
+    rc = lib().sd_oracle_run(len(h), _ptr(h), len(J), _ptr(u), _ptr(v), _ptr(J), R, _ptr(st),
+                             _ptr(en), _ptr(steps), 1 if large_sparse_opt else 0)
+    if rc < 0:
+        raise ValueError(f"oracle error {rc}")
+    return st, en, steps
+
+
+_ref_descent = None
+
+
+def reference_descent_module():
+    """The reference's steepest-descent extension built from source, or None."""
+    global _ref_descent
+    if _ref_descent is not None:
+        return _ref_descent
+    if not os.path.isdir(_REF_DIR):
+        return None
+    for name in os.listdir(_REF_DIR):
+        if name.startswith("descent") and name.endswith(".so"):
+            spec = importlib.util.spec_from_file_location("descent", os.path.join(_REF_DIR, name))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            _ref_descent = mod
+            return _ref_descent
+    return None
 
 
 def reference_module():

@@ -195,3 +195,90 @@ void sa_oracle_rng_stream(uint64_t seed, int count, uint64_t *out) {
     rng_seed(st, seed);
     for (int i = 0; i < count; i++) out[i] = rng_next(st);
 }
+
+/* ---- Steepest descent: dwave/samplers/greedy/src/descent.cpp ---------------
+ * The flip energy (descent.cpp:41-60) and the state energy (:75-93) are the
+ * same expressions as cpu_sa.cpp:54-74 and :210-227 above. */
+
+/* Linear-search solver, descent.cpp:117-187: flip the variable with the most
+ * negative flip energy (the first such index), update its neighbours with the
+ * NEW spin, until no flip energy is negative. */
+static unsigned sd_linear(int8_t *s, const double *h, const adjacency *a, double *fe) {
+    const int n = a->n;
+    if (n < 1) return 0;
+    for (int i = 0; i < n; i++) fe[i] = flip_energy(i, s, h, a);
+    unsigned steps = 0;
+    for (;;) {
+        int best = -1;
+        double best_e = 0;
+        for (int i = 0; i < n; i++)
+            if (fe[i] < best_e) {
+                best_e = fe[i];
+                best = i;
+            }
+        if (best < 0) break;
+        s[best] = (int8_t)(s[best] * -1);                        /* :168 */
+        fe[best] *= -1;                                          /* :172 */
+        for (int k = a->row[best]; k < a->row[best + 1]; k++) { /* :174-182 */
+            const int nb = a->col[k];
+            fe[nb] -= 4 * s[best] * a->w[k] * s[nb];
+        }
+        steps++;
+    }
+    return steps;
+}
+
+/* Ordered-set solver, descent.cpp:210-289: the same selection (least flip
+ * energy, ties to the lower index), neighbours updated with the OLD spin
+ * before the flip, and the flipped variable's entry then set to the negated
+ * value it had before the neighbour loop. */
+static unsigned sd_sparse(int8_t *s, const double *h, const adjacency *a, double *fe) {
+    const int n = a->n;
+    if (n < 1) return 0;
+    for (int i = 0; i < n; i++) fe[i] = flip_energy(i, s, h, a);
+    unsigned steps = 0;
+    for (;;) {
+        int best = 0;
+        double best_e = fe[0];
+        for (int i = 1; i < n; i++)
+            if (fe[i] < best_e) {
+                best_e = fe[i];
+                best = i;
+            }
+        if (best_e >= 0) break;                                  /* :244 */
+        for (int k = a->row[best]; k < a->row[best + 1]; k++) { /* :255-277 */
+            const int nb = a->col[k];
+            fe[nb] = fe[nb] + 4 * s[best] * a->w[k] * s[nb];
+        }
+        s[best] = (int8_t)(s[best] * -1);                        /* :280 */
+        fe[best] = best_e * -1;                                  /* :283-285 */
+        steps++;
+    }
+    return steps;
+}
+
+/* Driver, descent.cpp:315-405: each sample descends from its row of
+ * `states` (overwritten), then its energy; steps per sample. */
+int sd_oracle_run(int n, const double *h, long m, const int *u, const int *v,
+                  const double *J, int num_samples, int8_t *states, double *energies,
+                  unsigned *steps, int large_sparse_opt) {
+    adjacency a;
+    int rc = build_adjacency(&a, n, m, u, v, J);
+    if (rc) {
+        free_adjacency(&a);
+        return rc;
+    }
+    double *fe = (double *)malloc(sizeof(double) * ((size_t)n + 1));
+    if (!fe) {
+        free_adjacency(&a);
+        return ORACLE_ENOMEM;
+    }
+    for (int r = 0; r < num_samples; r++) {
+        int8_t *s = states + (size_t)r * (size_t)n;
+        steps[r] = large_sparse_opt ? sd_sparse(s, h, &a, fe) : sd_linear(s, h, &a, fe);
+        energies[r] = sa_oracle_energy(n, h, m, u, v, J, s);
+    }
+    free(fe);
+    free_adjacency(&a);
+    return num_samples;
+}

@@ -1,7 +1,8 @@
-"""Generate golden vectors from the reference's own simulated-annealing code.
+"""Generate golden vectors from the reference's own simulated-annealing and
+steepest-descent code.
 
-    bash oracle/build_ref.sh            # reference extension from its sources
-    python tests/golden/make_golden.py  # writes tests/golden/*.npz
+    bash oracle/build_ref.sh            # reference extensions from their sources
+    python tests/golden/make_golden.py  # writes tests/golden/*.npz, tests/golden/descent/*.npz
 
 Each fixture stores the inputs and the reference's outputs.  Per-read
 fixtures hold, for each read r, the result of one reference call with
@@ -170,6 +171,68 @@ def cases():
     return out
 
 
+def descent_cases():
+    """Steepest-descent fixtures: each runs in both solver modes.  The first
+    restates the reference test tests/test_greedy.py:26-45 (convex section of
+    a hyperbolic paraboloid).  No self-loops: a positive one makes the
+    reference descend for ever."""
+    rng = np.random.default_rng(20240602)
+    out = {"convex": dict(h=np.array([2.0, 2.0]), u=np.array([0]), v=np.array([1]),
+                          J=np.array([-1.0]), states0=np.array([[1, 1]], np.int8))}
+
+    def sparse(n, m, integer):
+        u = rng.integers(0, n, m)
+        v = rng.integers(0, n, m)
+        keep = u != v
+        u, v = u[keep], v[keep]
+        if integer:
+            return rng.integers(-2, 3, n).astype(float), u, v, rng.integers(-2, 3, len(u)).astype(float)
+        return rng.normal(0, 0.2, n), u, v, rng.normal(0, 1, len(u))
+
+    h, u, v, J = sparse(300, 900, False)
+    out["sparse300"] = dict(h=h, u=u, v=v, J=J, states0=states(rng, 32, 300))
+    h, u, v, J = sparse(120, 400, True)  # many equal flip energies: lowest index wins
+    out["integer_ties"] = dict(h=h, u=u, v=v, J=J, states0=states(rng, 32, 120))
+    n = 50
+    pairs = [(a, b) for a in range(n) for b in range(a + 1, n) if rng.random() < 0.1]
+    pairs = pairs + pairs[: len(pairs) // 3]  # repeated couplers
+    out["duplicates"] = dict(h=rng.normal(0, 0.3, n), u=np.array([p[0] for p in pairs]),
+                             v=np.array([p[1] for p in pairs]),
+                             J=rng.normal(0, 1, len(pairs)), states0=states(rng, 16, n))
+    n = 64
+    pairs = [(a, b) for a in range(n) for b in range(a + 1, n)]
+    out["dense64"] = dict(h=rng.uniform(-1, 1, n), u=np.array([p[0] for p in pairs]),
+                          v=np.array([p[1] for p in pairs]), J=rng.uniform(-1, 1, len(pairs)),
+                          states0=states(rng, 16, n))
+    h, u, v, J = sparse(2000, 6000, False)
+    out["sparse2000"] = dict(h=h, u=u, v=v, J=J, states0=states(rng, 8, 2000))
+    return out
+
+
+def main_descent():
+    mod = oracle.reference_descent_module()
+    if mod is None:
+        raise SystemExit("build the reference first: bash oracle/build_ref.sh")
+    outdir = os.path.join(HERE, "descent")
+    os.makedirs(outdir, exist_ok=True)
+    for name, c in descent_cases().items():
+        for mode in (False, True):
+            h = np.asarray(c["h"], np.float64)
+            u = np.asarray(c["u"], np.int32)
+            v = np.asarray(c["v"], np.int32)
+            J = np.asarray(c["J"], np.float64)
+            s0 = np.asarray(c["states0"], np.int8)
+            s, e, k = mod.steepest_gradient_descent(s0.shape[0], list(h), list(u), list(v),
+                                                    list(J), s0.copy(), mode)
+            tag = f"{name}_{'sparse' if mode else 'linear'}"
+            np.savez_compressed(os.path.join(outdir, f"{tag}.npz"), h=h, u=u, v=v, J=J,
+                                states0=s0, large_sparse_opt=np.array(mode),
+                                out_states=np.asarray(s, np.int8),
+                                out_energies=np.asarray(e, np.float64),
+                                out_steps=np.asarray(k, np.uint32))
+            print(f"descent/{tag}: samples={s0.shape[0]} n={len(h)} steps={int(np.sum(k))}")
+
+
 def main():
     if oracle.reference_module() is None:
         raise SystemExit("build the reference first: bash oracle/build_ref.sh")
@@ -189,3 +252,4 @@ def main():
 
 if __name__ == "__main__":
     main()
+    main_descent()
