@@ -72,6 +72,8 @@ def parse_args():
                     help="timed Boltzmann-machine gradient steps (after one untimed step)")
     ap.add_argument("--bm-target-reads", type=int, default=1024,
                     help="reads behind the BM target correlations (outside the timed steps)")
+    ap.add_argument("--descent-samples", type=int, default=4096,
+                    help="steepest-descent leg: samples (0 skips it)")
     return ap.parse_args()
 
 
@@ -304,6 +306,57 @@ def h2d_d2h_bytes(probs):
 
 # ------------------------------------------------------------------ arms ----
 
+def bench_descent(args, local, world, rank):
+    """Steepest descent (b200sa_steepest_descent, host buffers in and out,
+    linear-search solver) from uniform random states on a random 6-regular
+    Ising problem, n = 2048, J~N(0,1), h~N(0,0.1); one untimed call, then two
+    timed calls (host clock, max over ranks).  Rank 0 also times the
+    reference's own descent extension on all host threads over a bounded
+    sample of the same samples."""
+    import oracle
+    from b200sa.greedy import steepest_gradient_descent
+    rng = np.random.default_rng(17)
+    n, u, v = workloads.random_regular(2048, 6, rng, graph_seed=17)
+    J = rng.normal(0, 1, u.shape[0])
+    h = rng.normal(0, 0.1, n)
+    R = args.descent_samples
+    init = (2 * rng.integers(0, 2, (R, n)) - 1).astype(np.int8)
+    steepest_gradient_descent(R, h, u, v, J, init.copy(), False, device=local)
+    times, steps = [], 0
+    for _ in range(2):
+        st = init.copy()
+        t0 = time.perf_counter()
+        _, _, k = steepest_gradient_descent(R, h, u, v, J, st, False, device=local)
+        times.append(max_over_ranks(time.perf_counter() - t0, world, "cuda"))
+        steps = int(k.sum())
+    sec = statistics.median(times)
+    out = {"workload": "random 6-regular Ising, n=2048, J~N(0,1), h~N(0,0.1), uniform random "
+                       "initial states, linear-search solver",
+           "samples": R, "samples_per_s": world * R / sec, "flips_per_s": world * steps / sec,
+           "seconds": sec, "flips_per_sample": steps / R,
+           "note": "host buffers in and out (the call as a user makes it)"}
+    ref = oracle.reference_descent_module() if (rank == 0 and not args.no_cpu) else None
+    if ref is not None:
+        from concurrent.futures import ThreadPoolExecutor
+        threads = cpu_threads()
+        chunk = 8
+        sample = min(R, threads * chunk * 2)
+        hl, ul, vl, Jl = list(map(float, h)), list(map(int, u)), list(map(int, v)), list(map(float, J))
+
+        def one(i):  # the binding releases the GIL while descending (descent.pyx:102)
+            part = init[i:i + chunk].copy()
+            ref.steepest_gradient_descent(part.shape[0], hl, ul, vl, Jl, part, False)
+
+        with ThreadPoolExecutor(threads) as ex:
+            t0 = time.perf_counter()
+            list(ex.map(one, range(0, sample, chunk)))
+            cpu = time.perf_counter() - t0
+        out["cpu_reference"] = {"samples_per_s": sample / cpu, "cores": threads,
+                                "sample": f"{sample} of the same samples"}
+        out["gpu_over_cpu"] = out["samples_per_s"] / out["cpu_reference"]["samples_per_s"]
+    return out
+
+
 def bench_bm(args, local, world):
     """Batched Boltzmann-machine learning: 64 six-regular models, n~U[256,2048],
     ground truth J*~N(0,0.5), h*=0; per gradient step 1024 fixed-beta (beta=1)
@@ -489,6 +542,8 @@ def run_ours(args):
     del sin, sout, en
     if args.bm_steps > 0:
         line["bm"] = bench_bm(args, local, world)
+    if args.descent_samples > 0:
+        line["descent"] = bench_descent(args, local, world, rank)
 
     if rank == 0 and not args.no_cpu:
         cb = cpu_sample(probs, args.cpu_budget)
