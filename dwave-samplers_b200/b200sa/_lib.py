@@ -44,6 +44,7 @@ EXPORTS = (
     "b200sa_plan_set_weights",
     "b200sa_plan_autotune",
     "b200sa_steepest_descent",
+    "b200sa_rotor_anneal",
 )
 
 
@@ -176,6 +177,12 @@ def load() -> ctypes.CDLL:
         c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32,
         c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32, c.c_uint32, c.c_int32, c.c_char_p,
         c.c_size_t]
+    L.b200sa_rotor_anneal.restype = c.c_int
+    L.b200sa_rotor_anneal.argtypes = [
+        c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p,
+        c.c_int32, c.c_void_p, c.c_void_p, c.c_int32, c.c_int32, c.c_void_p, c.c_void_p,
+        c.c_void_p, c.c_int32, c.c_int32, c.c_int32, c.c_void_p, c.c_int32, c.c_int32,
+        c.POINTER(c.c_int64), c.c_char_p, c.c_size_t]
     L.b200sa_version.restype = c.c_char_p
     L.b200sa_version.argtypes = []
     _lib = L

@@ -11,6 +11,7 @@
 #include "sa_kernel.cuh"
 #include "sa_launch.h"
 #include "sd_kernel.cuh"
+#include "rmc_kernel.cuh"
 
 namespace b200sa {
 
@@ -244,6 +245,18 @@ cudaError_t sd_occupancy(bool sparse, bool smem, int warps_per_cta, int region_b
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, k, warps_per_cta * 32, bytes);
+}
+
+using RmcKernel = void (*)(RmcArgs);
+
+cudaError_t launch_rmc(bool random_order, int proposal, const RmcArgs &args, int grid,
+                       int block, cudaStream_t stream) {
+    static const RmcKernel table[2][4] = {
+        {rmc_kernel<false, 0>, rmc_kernel<false, 1>, rmc_kernel<false, 2>, rmc_kernel<false, 3>},
+        {rmc_kernel<true, 0>, rmc_kernel<true, 1>, rmc_kernel<true, 2>, rmc_kernel<true, 3>}};
+    if (proposal < 0 || proposal > 3) return cudaErrorInvalidValue;
+    table[random_order ? 1 : 0][proposal]<<<grid, block, 0, stream>>>(args);
+    return cudaGetLastError();
 }
 
 }  // namespace b200sa

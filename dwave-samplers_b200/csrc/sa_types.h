@@ -114,6 +114,32 @@ inline int sd_region_bytes(int cap_n) {
     return kSdScratchBytes + cap_n * 8 + ((cap_n + 15) & ~15);
 }
 
+// Arguments of the rotor-model annealing kernel (rmc_kernel.cuh).
+struct RmcArgs {
+    int32_t n;
+    int64_t m;
+    const uint2 *vinfo;      // [n] {list start, degree}
+    const int32_t *col;      // adjacency, coupler input order
+    const double *w;
+    const double *h;
+    const double *tf;        // [n] transverse fields
+    const int32_t *cu, *cv;  // COO (energy order)
+    const double *cw;
+    const double *hp, *hd;   // [num_betas] problem and driver field schedules
+    int32_t num_betas;
+    int32_t sweeps_per_beta;
+    const uint64_t *seeds;
+    int32_t shared_stream;   // 1: one thread, samples in order, one RNG stream
+    int32_t num_samples;
+    uint8_t *states;         // interleaved: element (v, r) at v * num_samples + r
+    double *de;              // interleaved like states
+    double *energies;
+    uint8_t *stats;          // [num_samples][points][n], or null
+    int32_t interval;
+    const double *cos_table, *sin_table;  // [256]
+    unsigned long long *near;
+};
+
 // Nibble tables of the RNG jump matrix: entry [k][v] is the jump applied to
 // the state whose only set bits are the nibble value v at nibble position k.
 constexpr int kJumpNibbles = 32;

@@ -216,6 +216,37 @@ B200SA_API int b200sa_steepest_descent(int32_t num_vars, const double *h, int64_
                                        int32_t large_sparse_opt, uint32_t max_steps,
                                        int32_t device, char *err, size_t errlen);
 
+/* ---- Rotor-model annealing (SQA) -------------------------------------------
+ * Replaces general_simulated_annealing of the rotor Monte Carlo
+ * (dwave/samplers/sqa/src/cpu_rotormc.cpp:368-563, cpu_rotormc.h; bound at
+ * dwave/samplers/sqa/rotormc_annealing.pyx:54-236).  States are uint8 angles
+ * (theta = 2*pi*index/256), host arrays, num_samples x num_vars, overwritten.
+ * hp_field / hd_field: num_betas problem and driver inverse temperatures;
+ * trans_fields: num_vars transverse fields.  proposal: 0 GibbsNonErgodic,
+ * 1 MetropolisNonErgodic, 2 MetropolisUniform, 3 MetropolisTF (the
+ * reference's enum order).  seeds: num_seeds == 1 continues one stream over
+ * the samples exactly as one reference call (samples then run one after
+ * another); num_seeds == num_samples makes sample r equal a reference call
+ * with num_samples = 1 and seed = seeds[r] (samples run in parallel).
+ * statistics (NULL: none) receives, for schedule_sample_interval > 0, the
+ * state after every beta index divisible by the interval: num_samples blocks
+ * of num_vars * (1 + (num_betas - 1) / interval) bytes, laid out as the
+ * reference's call lays them out (with one stream, sample r's block starts at
+ * r * num_vars * (num_betas / interval)).  near_ties (optional) counts
+ * exp() decisions within 2^-48 of the threshold (expected 0).  Returns
+ * num_samples or a negative error. */
+B200SA_API int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t num_couplers,
+                                   const int32_t *coupler_starts, const int32_t *coupler_ends,
+                                   const double *coupler_weights, const double *trans_fields,
+                                   int32_t num_samples, uint8_t *states, double *energies,
+                                   int32_t sweeps_per_beta, int32_t num_betas,
+                                   const double *hp_field, const double *hd_field,
+                                   const uint64_t *seeds, int32_t num_seeds,
+                                   int32_t randomize_order, int32_t proposal,
+                                   uint8_t *statistics, int32_t schedule_sample_interval,
+                                   int32_t device, int64_t *near_ties, char *err,
+                                   size_t errlen);
+
 /* ---- Sample moments (no reference counterpart) ------------------------------
  * For the gradient of log Z of p(s) ~ exp(-beta*E(s)), E as in cpu_sa.cpp:210-227:
  * d log Z/d h_i = -beta <s_i>, d log Z/d J_c = -beta <s_u(c) s_v(c)>.  Adds the

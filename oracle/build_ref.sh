@@ -55,3 +55,17 @@ if [ -f "$GR/descent.pyx" ]; then
     rm -f "$OUT/descent.cpp"
     echo "built $OUT/descent$EXT_SUFFIX"
 fi
+
+# The reference's rotor-model annealing extension (SQA):
+#   <ref>/dwave/samplers/sqa/rotormc_annealing.pyx, src/cpu_rotormc.cpp, .h
+SQ="$REF/dwave/samplers/sqa"
+if [ -f "$SQ/rotormc_annealing.pyx" ]; then
+    $PY -m cython --cplus -3 -Xfreethreading_compatible=True -I "$REF" \
+        -o "$OUT/rotormc_annealing.cpp" "$SQ/rotormc_annealing.pyx"
+    g++ -O3 -std=c++17 -g1 -DNDEBUG -fPIC -shared -Wall -Wno-unused-function \
+        -I"$SQ/src" -I"$PYINC" -I"$NPINC" \
+        "$OUT/rotormc_annealing.cpp" "$SQ/src/cpu_rotormc.cpp" \
+        -o "$OUT/rotormc_annealing$EXT_SUFFIX"
+    rm -f "$OUT/rotormc_annealing.cpp"
+    echo "built $OUT/rotormc_annealing$EXT_SUFFIX"
+fi

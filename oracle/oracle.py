@@ -11,6 +11,9 @@ Two oracles are exposed:
 * :func:`reference_module` -- the reference's own Cython extension
   (``dwave/samplers/sa/simulated_annealing.pyx``) built from its sources by
   ``oracle/build_ref.sh`` into ``oracle/_ref/``, when that build exists.
+* :func:`rotormc` -- the C restatement of the reference's rotor-model
+  (SQA) annealing (``dwave/samplers/sqa/src/cpu_rotormc.cpp:368-563``), and
+  :func:`reference_rotormc_module`, its own extension built the same way.
 * :func:`descent` -- the C restatement of the reference's steepest descent
   (``dwave/samplers/greedy/src/descent.cpp:315-405``), and
   :func:`reference_descent_module`, the reference's own ``descent`` extension
@@ -63,6 +66,12 @@ def lib() -> ctypes.CDLL:
             ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.rmc_oracle_run.restype = ctypes.c_int
+        L.rmc_oracle_run.argtypes = [
+            ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
         L.sa_oracle_rng_stream.restype = None
         L.sa_oracle_rng_stream.argtypes = [ctypes.c_uint64, ctypes.c_int,
                                            ctypes.c_void_p]
@@ -135,6 +144,60 @@ def descent(h, u, v, J, states, large_sparse_opt=False):
     if rc < 0:
         raise ValueError(f"oracle error {rc}")
     return st, en, steps
+
+
+ROTOR_PROPOSALS = {"GibbsNonErgodic": 0, "MetropolisNonErgodic": 1, "MetropolisUniform": 2,
+                   "MetropolisTF": 3}
+
+
+def rotormc(h, u, v, J, trans_fields, states, sweeps_per_beta, hp, hd, seeds,
+            randomize_order=False, proposal="MetropolisNonErgodic", interval=0):
+    """Rotor-model annealing of every row of ``states`` (uint8 angles, copied).
+    ``seeds``: one seed (one stream across samples) or one per sample.  Returns
+    (states, energies, statistics) with statistics (samples, points, n), one
+    block per sample."""
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.int32)
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    tf = np.ascontiguousarray(trans_fields, dtype=np.float64)
+    hp = np.ascontiguousarray(hp, dtype=np.float64)
+    hd = np.ascontiguousarray(hd, dtype=np.float64)
+    seeds = np.atleast_1d(np.asarray(seeds, dtype=np.uint64))
+    st = np.array(states, dtype=np.uint8, order="C", copy=True)
+    R, n = st.shape
+    en = np.zeros(R, dtype=np.float64)
+    points = 1 + (len(hp) - 1) // interval if interval else 0
+    stats = np.zeros((R, max(points, 1), n), dtype=np.uint8)
+    rc = lib().rmc_oracle_run(n, _ptr(h), len(J), _ptr(u), _ptr(v), _ptr(J), _ptr(tf), R,
+                              _ptr(st), _ptr(en), int(sweeps_per_beta), len(hp), _ptr(hp),
+                              _ptr(hd), _ptr(seeds), len(seeds), 1 if randomize_order else 0,
+                              ROTOR_PROPOSALS[proposal], _ptr(stats) if interval else None,
+                              int(interval))
+    if rc < 0:
+        raise ValueError(f"oracle error {rc}")
+    return st, en, stats[:, :points]
+
+
+_ref_rotormc = None
+
+
+def reference_rotormc_module():
+    """The reference's rotor-model annealing extension built from source, or None."""
+    global _ref_rotormc
+    if _ref_rotormc is not None:
+        return _ref_rotormc
+    if not os.path.isdir(_REF_DIR):
+        return None
+    for name in os.listdir(_REF_DIR):
+        if name.startswith("rotormc_annealing") and name.endswith(".so"):
+            spec = importlib.util.spec_from_file_location(
+                "rotormc_annealing", os.path.join(_REF_DIR, name))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            _ref_rotormc = mod
+            return _ref_rotormc
+    return None
 
 
 _ref_descent = None

@@ -282,3 +282,156 @@ int sd_oracle_run(int n, const double *h, long m, const int *u, const int *v,
     free_adjacency(&a);
     return num_samples;
 }
+
+/* ---- Rotor-model annealing (SQA): dwave/samplers/sqa/src/cpu_rotormc.cpp ----
+ * States are uint8 angles theta = 2*pi*index/256, with cos and |sin| tables
+ * computed as at cpu_rotormc.cpp:377-383.  Proposals (cpu_rotormc.h enum):
+ * 0 GibbsNonErgodic, 1 MetropolisNonErgodic, 2 MetropolisUniform,
+ * 3 MetropolisTF. */
+
+static const double RMC_PI = 3.14159265358979323846; /* M_PI */
+
+static void rmc_tables(double *c, double *s) {
+    for (int i = 0; i < 256; i++) {
+        c[i] = cos(2 * i * RMC_PI / 256);
+        s[i] = fabs(sin(2 * i * RMC_PI / 256));
+    }
+}
+
+/* cpu_rotormc.cpp:46-60: h plus cos(neighbour angle) * J, adjacency order. */
+static double rmc_field(int var, const uint8_t *st, const double *h, const adjacency *a,
+                        const double *cs) {
+    double e = h[var];
+    for (int k = a->row[var]; k < a->row[var + 1]; k++) e += cs[st[a->col[k]]] * a->w[k];
+    return e;
+}
+
+/* One run, cpu_rotormc.cpp:104-296.  `stats` receives the state after every
+ * beta index divisible by `interval` (interval 0: none). */
+static void rmc_run(uint8_t *st, const double *h, const adjacency *a, const double *tf,
+                    int spb, int nb, const double *hp, const double *hd, int order,
+                    int proposal, const double *cs, const double *sn, uint64_t rng[2],
+                    double *de, uint8_t *stats, int interval) {
+    const int n = a->n;
+    for (int v = 0; v < n; v++) de[v] = rmc_field(v, st, h, a, cs);
+    if (proposal <= 1)
+        for (int v = 0; v < n; v++) de[v] *= -2 * cs[st[v]];
+    for (int i = 0; i < 32; i++) rng_next(rng); /* :141-143 burn-in */
+    for (int b = 0; b < nb; b++) {
+        const double beta = hp[b], beta_tf = hd[b];
+        const double rat = beta_tf / beta;
+        for (int sw = 0; sw < spb; sw++) {
+            for (int i = 0; i < n; i++) {
+                int var = i;
+                if (order) var = (int)(rng_next(rng) % (uint64_t)n);
+                uint8_t prop = 0;
+                double prop_e = 0.0;
+                int flip = 0;
+                if (proposal == 1) { /* :167-184 */
+                    prop = (uint8_t)(128 + st[var]);
+                    prop_e = -de[var];
+                    if (de[var] <= 0.0) {
+                        flip = 1;
+                    } else {
+                        const uint64_t r = rng_next(rng);
+                        if (exp(-de[var] * beta) * RANDMAX_D > (double)r) flip = 1;
+                    }
+                } else if (proposal == 0) { /* :185-196 */
+                    prop = (uint8_t)(128 + st[var]);
+                    prop_e = -de[var];
+                    const uint64_t r = rng_next(rng);
+                    if (RANDMAX_D > (double)r * (1 + exp(de[var] * beta))) flip = 1;
+                } else {
+                    uint64_t r = rng_next(rng);
+                    if (proposal == 2 || rat >= 1) { /* :197-200, 206-207 */
+                        prop = (uint8_t)(r % 256);
+                    } else { /* :208-233 */
+                        const int osi = (int)(rat * 128 - 0.5);
+                        const double distc = (osi * (osi + 1)) / (double)(2 * osi + 1);
+                        const double p = (rat / 2 * 128 - distc) / (osi + 1 - distc);
+                        const uint64_t rl = r;
+                        r = rng_next(rng);
+                        const uint8_t pac = (p * RANDMAX_D > (double)rl)
+                                                ? (uint8_t)((uint64_t)(osi + 1) * (2 * (r % 2) - 1))
+                                                : (uint8_t)(r % (uint64_t)(2 * osi + 1) - (uint64_t)osi);
+                        prop = (uint8_t)(st[var] + pac);
+                    }
+                    /* :244-266 */
+                    prop_e = rmc_field(var, st, h, a, cs);
+                    const double dlm = -beta * prop_e * (cs[prop] - cs[st[var]]) +
+                                       beta_tf * tf[var] * (sn[prop] - sn[st[var]]);
+                    if (dlm >= 0.0) {
+                        flip = 1;
+                    } else {
+                        const uint64_t r2 = rng_next(rng);
+                        if (exp(dlm) * RANDMAX_D > (double)r2) flip = 1;
+                    }
+                }
+                if (flip) { /* :268-287 */
+                    if (proposal <= 1) {
+                        const double mult = 2 * (cs[st[var]] - cs[prop]);
+                        for (int k = a->row[var]; k < a->row[var + 1]; k++) {
+                            const int nbv = a->col[k];
+                            de[nbv] += mult * a->w[k] * cs[st[nbv]];
+                        }
+                        de[var] = prop_e;
+                    }
+                    st[var] = prop;
+                }
+            }
+        }
+        if (interval != 0 && b % interval == 0) { /* :289-293 */
+            memcpy(stats, st, (size_t)n);
+            stats += n;
+        }
+    }
+}
+
+/* cpu_rotormc.cpp:310-326: cos-weighted classical energy. */
+static double rmc_energy(int n, const double *h, long m, const int *u, const int *v,
+                         const double *J, const uint8_t *st, const double *cs) {
+    double e = 0.0;
+    for (int i = 0; i < n; i++) e += cs[st[i]] * h[i];
+    for (long c = 0; c < m; c++) e += cs[st[u[c]]] * J[c] * cs[st[v[c]]];
+    return e;
+}
+
+/* Driver, cpu_rotormc.cpp:368-563.  num_seeds 1: one stream across samples
+ * (the reference's call); num_seeds == num_samples: sample r as its own call
+ * with seed seeds[r].  `stats` holds num_samples blocks of
+ * n * (1 + (num_betas - 1) / interval) bytes, one per sample (the reference's
+ * own buffer places sample r at r * n * (num_betas / interval); the caller
+ * rearranges). */
+int rmc_oracle_run(int n, const double *h, long m, const int *u, const int *v,
+                   const double *J, const double *tf, int num_samples, uint8_t *states,
+                   double *energies, int spb, int nb, const double *hp, const double *hd,
+                   const uint64_t *seeds, int num_seeds, int order, int proposal,
+                   uint8_t *stats, int interval) {
+    if (proposal < 0 || proposal > 3) return ORACLE_EINVAL;
+    adjacency a;
+    int rc = build_adjacency(&a, n, m, u, v, J);
+    if (rc) {
+        free_adjacency(&a);
+        return rc;
+    }
+    double cs[256], sn[256];
+    rmc_tables(cs, sn);
+    double *de = (double *)malloc(sizeof(double) * ((size_t)n + 1));
+    if (!de) {
+        free_adjacency(&a);
+        return ORACLE_ENOMEM;
+    }
+    const long points = interval ? 1 + (nb - 1) / interval : 0;
+    uint64_t rng[2] = {0, 0};
+    if (num_seeds == 1) rng_seed(rng, seeds[0]);
+    for (int r = 0; r < num_samples; r++) {
+        if (num_seeds != 1) rng_seed(rng, seeds[r]);
+        uint8_t *st = states + (size_t)r * (size_t)n;
+        rmc_run(st, h, &a, tf, spb, nb, hp, hd, order, proposal, cs, sn, rng, de,
+                stats ? stats + (size_t)r * (size_t)points * (size_t)n : NULL, stats ? interval : 0);
+        energies[r] = rmc_energy(n, h, m, u, v, J, st, cs);
+    }
+    free(de);
+    free_adjacency(&a);
+    return num_samples;
+}

@@ -233,6 +233,58 @@ def main_descent():
             print(f"descent/{tag}: samples={s0.shape[0]} n={len(h)} steps={int(np.sum(k))}")
 
 
+def rotor_cases():
+    """Rotor-model (SQA) fixtures: every proposal in both orders, statistics
+    on, per-sample calls and one continued-stream call."""
+    rng = np.random.default_rng(20240603)
+    out = {}
+    n = 40
+    pairs = [(a, b) for a in range(n) for b in range(a + 1, n) if rng.random() < 0.15]
+    base = dict(h=rng.normal(0, 0.5, n), u=np.array([p[0] for p in pairs]),
+                v=np.array([p[1] for p in pairs]), J=rng.normal(0, 1, len(pairs)),
+                tf=rng.uniform(0.1, 2.0, n), spb=2, hp=np.geomspace(0.05, 4.0, 11),
+                hd=np.geomspace(4.0, 0.02, 11), interval=3)
+    for prop in ("GibbsNonErgodic", "MetropolisNonErgodic", "MetropolisUniform", "MetropolisTF"):
+        for order in (False, True):
+            for shared in (False, True):
+                c = dict(base)
+                c.update(states0=rng.integers(0, 256, (6, n)).astype(np.uint8),
+                         seed=int(rng.integers(0, 2**31)), order=order, proposal=prop,
+                         shared=shared)
+                out[f"{prop}_{'random' if order else 'seq'}_{'shared' if shared else 'per_read'}"] = c
+    return out
+
+
+def main_rotor():
+    mod = oracle.reference_rotormc_module()
+    if mod is None:
+        raise SystemExit("build the reference first: bash oracle/build_ref.sh")
+    outdir = os.path.join(HERE, "rotor")
+    os.makedirs(outdir, exist_ok=True)
+    for name, c in rotor_cases().items():
+        args = (list(map(float, c["h"])), list(map(int, c["u"])), list(map(int, c["v"])),
+                list(map(float, c["J"])), list(map(float, c["tf"])), c["spb"], c["hp"], c["hd"])
+        s0 = c["states0"]
+        if c["shared"]:
+            s, e, st = mod.simulated_annealing(s0.shape[0], *args, c["seed"], s0.copy(),
+                                               c["order"], c["proposal"], c["interval"])
+            s, e, st = np.asarray(s), np.asarray(e), np.asarray(st)
+        else:
+            outs = [mod.simulated_annealing(1, *args, c["seed"] + r, s0[r:r + 1].copy(),
+                                            c["order"], c["proposal"], c["interval"])
+                    for r in range(s0.shape[0])]
+            s = np.concatenate([np.asarray(o[0]) for o in outs])
+            e = np.concatenate([np.asarray(o[1]) for o in outs])
+            st = np.concatenate([np.asarray(o[2]) for o in outs])
+        np.savez_compressed(os.path.join(outdir, f"{name}.npz"), h=c["h"], u=c["u"].astype(np.int32),
+                            v=c["v"].astype(np.int32), J=c["J"], tf=c["tf"], spb=c["spb"],
+                            hp=c["hp"], hd=c["hd"], interval=c["interval"], states0=s0,
+                            seed=np.uint64(c["seed"]), order=c["order"], proposal=c["proposal"],
+                            shared=c["shared"], out_states=s.astype(np.uint8),
+                            out_energies=e.astype(np.float64), out_stats=st.astype(np.uint8))
+        print(f"rotor/{name}: samples={s0.shape[0]} n={len(c['h'])}")
+
+
 def main():
     if oracle.reference_module() is None:
         raise SystemExit("build the reference first: bash oracle/build_ref.sh")
@@ -253,3 +305,4 @@ def main():
 if __name__ == "__main__":
     main()
     main_descent()
+    main_rotor()
