@@ -74,6 +74,8 @@ def parse_args():
                     help="reads behind the BM target correlations (outside the timed steps)")
     ap.add_argument("--descent-samples", type=int, default=4096,
                     help="steepest-descent leg: samples (0 skips it)")
+    ap.add_argument("--rotor-samples", type=int, default=4096,
+                    help="rotor-model (SQA) annealing leg: samples (0 skips it)")
     return ap.parse_args()
 
 
@@ -357,6 +359,62 @@ def bench_descent(args, local, world, rank):
     return out
 
 
+def bench_rotor(args, local, world, rank):
+    """Rotor-model (SQA) annealing (b200sa_rotor_anneal, host buffers,
+    MetropolisNonErgodic, sequential order, per-sample seeds) on a random
+    6-regular problem, n = 512, J~N(0,1), h~N(0,0.1), transverse fields
+    U[0.5, 1.5], 64 sweeps of geometric schedules (problem 0.1 -> 5,
+    driver 5 -> 0.05), uniform random angles; one untimed call, then two
+    timed calls.  Rank 0 also times the reference's own extension (one call
+    per sample, seed + r) on all host threads over a bounded sample."""
+    import oracle
+    from b200sa.sqa import simulated_annealing as rotor
+    rng = np.random.default_rng(29)
+    n, u, v = workloads.random_regular(512, 6, rng, graph_seed=29)
+    J = rng.normal(0, 1, u.shape[0])
+    h = rng.normal(0, 0.1, n)
+    tf = rng.uniform(0.5, 1.5, n)
+    hp = np.geomspace(0.1, 5.0, 64)
+    hd = np.geomspace(5.0, 0.05, 64)
+    R = args.rotor_samples
+    init = rng.integers(0, 256, (R, n)).astype(np.uint8)
+    call = lambda st: rotor(R, h, u, v, J, tf, 1, hp, hd, 1234, st, False,
+                            "MetropolisNonErgodic", 0, device=local)
+    call(init.copy())
+    times = []
+    for _ in range(2):
+        st = init.copy()
+        t0 = time.perf_counter()
+        call(st)
+        times.append(max_over_ranks(time.perf_counter() - t0, world, "cuda"))
+    sec = statistics.median(times)
+    attempts = R * n * len(hp)
+    out = {"workload": "rotor model, random 6-regular n=512, J~N(0,1), h~N(0,0.1), transverse "
+                       "fields U[0.5,1.5], 64 sweeps, MetropolisNonErgodic, sequential order",
+           "samples": R, "attempts_per_s": world * attempts / sec, "seconds": sec,
+           "note": "host buffers in and out (the call as a user makes it)"}
+    ref = oracle.reference_rotormc_module() if (rank == 0 and not args.no_cpu) else None
+    if ref is not None:
+        from concurrent.futures import ThreadPoolExecutor
+        threads = cpu_threads()
+        sample = min(R, threads * 4)
+        args_ref = (list(map(float, h)), list(map(int, u)), list(map(int, v)),
+                    list(map(float, J)), list(map(float, tf)), 1, hp, hd)
+
+        def one(r):  # one call per sample, seed + r; the binding releases the GIL
+            ref.simulated_annealing(1, *args_ref, 1234 + r, init[r:r + 1].copy(), False,
+                                    "MetropolisNonErgodic", 0)
+
+        with ThreadPoolExecutor(threads) as ex:
+            t0 = time.perf_counter()
+            list(ex.map(one, range(sample)))
+            cpu = time.perf_counter() - t0
+        out["cpu_reference"] = {"attempts_per_s": sample * n * len(hp) / cpu, "cores": threads,
+                                "sample": f"{sample} of the same samples"}
+        out["gpu_over_cpu"] = out["attempts_per_s"] / out["cpu_reference"]["attempts_per_s"]
+    return out
+
+
 def bench_bm(args, local, world):
     """Batched Boltzmann-machine learning: 64 six-regular models, n~U[256,2048],
     ground truth J*~N(0,0.5), h*=0; per gradient step 1024 fixed-beta (beta=1)
@@ -544,6 +602,8 @@ def run_ours(args):
         line["bm"] = bench_bm(args, local, world)
     if args.descent_samples > 0:
         line["descent"] = bench_descent(args, local, world, rank)
+    if args.rotor_samples > 0:
+        line["rotor"] = bench_rotor(args, local, world, rank)
 
     if rank == 0 and not args.no_cpu:
         cb = cpu_sample(probs, args.cpu_budget)
