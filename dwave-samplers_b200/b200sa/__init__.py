@@ -1,13 +1,20 @@
-"""b200sa: the simulated-annealing sweep of dwave-samplers, on B200 (sm_100a).
+"""b200sa: the simulated-annealing path of dwave-samplers, on B200 (sm_100a).
 
-Public surface (mirrors ``dwave.samplers.sa``):
+Public surface:
 
 * :func:`simulated_annealing` -- the Cython-level drop-in
   (``dwave/samplers/sa/simulated_annealing.pyx``).
-* :func:`sample_batch`, :class:`Plan` -- many problems in one persistent launch.
+* :func:`sample_batch`, :class:`Plan` -- many problems in one persistent
+  launch (graph replay, in-place weights, autotuning).
+* :mod:`b200sa.sampler` -- ``SimulatedAnnealingSampler`` front end (dimod-free).
+* :mod:`b200sa.greedy` -- steepest descent (``dwave.samplers.greedy``).
+* :mod:`b200sa.sqa` -- rotor-model annealing (``dwave.samplers.sqa``'s rotor
+  Monte Carlo binding).
+* :mod:`b200sa.autograd`, :mod:`b200sa.bm` -- differentiable fixed-beta
+  sampling and batched Boltzmann-machine learning.
 """
 from .simulated_annealing import per_read_seeds, simulated_annealing
 from .batch import Plan, sample_batch
 
 __all__ = ["simulated_annealing", "per_read_seeds", "sample_batch", "Plan"]
-__version__ = "0.1.0"
+__version__ = "0.4.0"
