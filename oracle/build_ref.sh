@@ -1,7 +1,7 @@
 #!/usr/bin/env bash
-# Build the reference's own simulated-annealing and steepest-descent
-# extensions from their sources, for use as test oracles and as the timed CPU
-# baseline.  Test infrastructure only.
+# Build the reference's own simulated-annealing, steepest-descent and SQA
+# (rotor and path-integral) extensions from their sources, for use as test
+# oracles and as the timed CPU baseline.  Test infrastructure only.
 #
 # Sources (read in place, never copied into the repository):
 #   <ref>/dwave/samplers/sa/simulated_annealing.pyx   (Cython binding)
@@ -68,4 +68,17 @@ if [ -f "$SQ/rotormc_annealing.pyx" ]; then
         -o "$OUT/rotormc_annealing$EXT_SUFFIX"
     rm -f "$OUT/rotormc_annealing.cpp"
     echo "built $OUT/rotormc_annealing$EXT_SUFFIX"
+fi
+
+# The reference's path-integral Monte Carlo extension (SQA):
+#   <ref>/dwave/samplers/sqa/pimc_annealing.pyx, src/localPIMC.cpp, .h
+if [ -f "$SQ/pimc_annealing.pyx" ]; then
+    $PY -m cython --cplus -3 -Xfreethreading_compatible=True -I "$REF" \
+        -o "$OUT/pimc_annealing.cpp" "$SQ/pimc_annealing.pyx"
+    g++ -O3 -std=c++17 -g1 -DNDEBUG -fPIC -shared -Wall -Wno-unused-function \
+        -Wno-sign-compare -I"$SQ/src" -I"$PYINC" -I"$NPINC" \
+        "$OUT/pimc_annealing.cpp" "$SQ/src/localPIMC.cpp" \
+        -o "$OUT/pimc_annealing$EXT_SUFFIX"
+    rm -f "$OUT/pimc_annealing.cpp"
+    echo "built $OUT/pimc_annealing$EXT_SUFFIX"
 fi

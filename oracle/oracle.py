@@ -14,6 +14,9 @@ Two oracles are exposed:
 * :func:`rotormc` -- the C restatement of the reference's rotor-model
   (SQA) annealing (``dwave/samplers/sqa/src/cpu_rotormc.cpp:368-563``), and
   :func:`reference_rotormc_module`, its own extension built the same way.
+* :func:`pimc` -- the C restatement of the reference's path-integral Monte
+  Carlo annealing (``dwave/samplers/sqa/src/localPIMC.cpp``), with
+  :func:`mt19937`, and :func:`reference_pimc_module`, its own extension.
 * :func:`descent` -- the C restatement of the reference's steepest descent
   (``dwave/samplers/greedy/src/descent.cpp:315-405``), and
   :func:`reference_descent_module`, the reference's own ``descent`` extension
@@ -39,9 +42,9 @@ _ref = None
 
 def build() -> str:
     """Compile the C restatement (plain gcc) if it is missing or stale."""
-    src = os.path.join(HERE, "sa_oracle.c")
+    srcs = [os.path.join(HERE, f) for f in ("sa_oracle.c", "pimc_oracle.c")]
     if (not os.path.exists(_LIB_PATH)
-            or os.path.getmtime(_LIB_PATH) < os.path.getmtime(src)):
+            or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs))):
         subprocess.check_call(["make", "-s", "-C", HERE, "libsa_oracle.so"])
     return _LIB_PATH
 
@@ -72,6 +75,15 @@ def lib() -> ctypes.CDLL:
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        L.pimc_oracle_run.restype = ctypes.c_int
+        L.pimc_oracle_run.argtypes = [
+            ctypes.c_int, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+            ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int,
+            ctypes.c_int, ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        L.pimc_oracle_mt.restype = None
+        L.pimc_oracle_mt.argtypes = [ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p]
         L.sa_oracle_rng_stream.restype = None
         L.sa_oracle_rng_stream.argtypes = [ctypes.c_uint64, ctypes.c_int,
                                            ctypes.c_void_p]
@@ -177,6 +189,70 @@ def rotormc(h, u, v, J, trans_fields, states, sweeps_per_beta, hp, hd, seeds,
     if rc < 0:
         raise ValueError(f"oracle error {rc}")
     return st, en, stats[:, :points]
+
+
+def pimc(h, u, v, J, states, sweeps_per_beta, hp, hd, seed, chain_coupler_strength=1.0,
+         qubits_per_chain=1, qubits_per_update=1, project_inputs=True, project_outputs=True,
+         num_breaks=None, breaks_in=None, interval=0, max_out=64):
+    """Path-integral Monte Carlo annealing of every row of ``states`` (int8,
+    copied) as ONE reference call (one mt19937 stream across the samples).
+    Returns (states, energies, statistics (samples, points, n), num_breaks
+    (samples, n), breaks (samples, n, max_out): the final break positions of
+    every variable, valid up to num_breaks)."""
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.int32)
+    v = np.ascontiguousarray(v, dtype=np.int32)
+    J = np.ascontiguousarray(J, dtype=np.float64)
+    hp = np.ascontiguousarray(hp, dtype=np.float64)
+    hd = np.ascontiguousarray(hd, dtype=np.float64)
+    st = np.array(states, dtype=np.int8, order="C", copy=True)
+    R, n = st.shape
+    en = np.zeros(R, dtype=np.float64)
+    points = 1 + (len(hp) - 1) // interval if interval else 0
+    stats = np.zeros((R, max(points, 1), n), dtype=np.int8)
+    nbk = (np.zeros((R, n), dtype=np.int32) if num_breaks is None
+           else np.array(num_breaks, dtype=np.int32, order="C", copy=True))
+    bin_ = np.ascontiguousarray(np.zeros(1) if breaks_in is None else breaks_in, dtype=np.int32)
+    bout = np.zeros((R, n, max_out), dtype=np.int32)
+    rc = lib().pimc_oracle_run(n, _ptr(h), len(J), _ptr(u), _ptr(v), _ptr(J), R, _ptr(st),
+                               _ptr(en), int(sweeps_per_beta), len(hp), _ptr(hp), _ptr(hd),
+                               float(chain_coupler_strength), int(qubits_per_chain),
+                               int(qubits_per_update), int(seed), 1 if project_inputs else 0,
+                               1 if project_outputs else 0, _ptr(nbk), _ptr(bin_), _ptr(bout),
+                               int(max_out), _ptr(stats) if interval else None, int(interval))
+    if rc == -2:
+        raise ValueError("a variable ended with more than max_out breaks")
+    if rc < 0:
+        raise ValueError(f"oracle error {rc}")
+    return st, en, stats[:, :points], nbk, bout
+
+
+def mt19937(seed, count):
+    """First ``count`` outputs of std::mt19937(seed) as restated by the oracle."""
+    out = np.zeros(count, dtype=np.uint32)
+    lib().pimc_oracle_mt(int(seed), int(count), _ptr(out))
+    return out
+
+
+_ref_pimc = None
+
+
+def reference_pimc_module():
+    """The reference's path-integral annealing extension built from source, or None."""
+    global _ref_pimc
+    if _ref_pimc is not None:
+        return _ref_pimc
+    if not os.path.isdir(_REF_DIR):
+        return None
+    for name in os.listdir(_REF_DIR):
+        if name.startswith("pimc_annealing") and name.endswith(".so"):
+            spec = importlib.util.spec_from_file_location(
+                "pimc_annealing", os.path.join(_REF_DIR, name))
+            mod = importlib.util.module_from_spec(spec)
+            spec.loader.exec_module(mod)
+            _ref_pimc = mod
+            return _ref_pimc
+    return None
 
 
 _ref_rotormc = None
