@@ -18,6 +18,7 @@ ECUDA = -2
 ENOMEM = -3
 ENODEV = -4
 ETIMEOUT = -5
+ERANGE = -6
 
 GIBBS = 0
 METROPOLIS = 1
@@ -45,6 +46,7 @@ EXPORTS = (
     "b200sa_plan_autotune",
     "b200sa_steepest_descent",
     "b200sa_rotor_anneal",
+    "b200sa_path_anneal",
 )
 
 
@@ -183,10 +185,22 @@ def load() -> ctypes.CDLL:
         c.c_int32, c.c_void_p, c.c_void_p, c.c_int32, c.c_int32, c.c_void_p, c.c_void_p,
         c.c_void_p, c.c_int32, c.c_int32, c.c_int32, c.c_void_p, c.c_int32, c.c_int32,
         c.POINTER(c.c_int64), c.c_char_p, c.c_size_t]
+    L.b200sa_path_anneal.restype = c.c_int
+    L.b200sa_path_anneal.argtypes = [
+        c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32,
+        c.c_void_p, c.c_void_p, c.c_int32, c.c_int32, c.c_void_p, c.c_void_p, c.c_double,
+        c.c_int32, c.c_int32, c.c_void_p, c.c_int32, c.c_int32, c.c_int32, c.c_void_p,
+        c.c_void_p, c.c_int64, c.c_void_p, c.c_int64, c.c_void_p, c.c_int32, c.c_int32,
+        c.c_int32, c.POINTER(c.c_int64), c.c_char_p, c.c_size_t]
     L.b200sa_version.restype = c.c_char_p
     L.b200sa_version.argtypes = []
     _lib = L
     return L
+
+
+class CapacityError(RuntimeError):
+    """A fixed device capacity (break lists of path-integral annealing) was
+    exceeded; calling again with a larger capacity succeeds."""
 
 
 def check(rc: int, err: ctypes.Array) -> int:
@@ -200,6 +214,8 @@ def check(rc: int, err: ctypes.Array) -> int:
         raise MemoryError(msg or "out of memory")
     if rc == ETIMEOUT:
         raise TimeoutError(msg or "device wait timed out")
+    if rc == ERANGE:
+        raise CapacityError(msg or "capacity exceeded")
     raise RuntimeError(f"b200sa error {rc}: {msg}")
 
 

@@ -12,6 +12,7 @@
 #include "sa_launch.h"
 #include "sd_kernel.cuh"
 #include "rmc_kernel.cuh"
+#include "pimc_kernel.cuh"
 
 namespace b200sa {
 
@@ -256,6 +257,15 @@ cudaError_t launch_rmc(bool random_order, int proposal, const RmcArgs &args, int
         {rmc_kernel<true, 0>, rmc_kernel<true, 1>, rmc_kernel<true, 2>, rmc_kernel<true, 3>}};
     if (proposal < 0 || proposal > 3) return cudaErrorInvalidValue;
     table[random_order ? 1 : 0][proposal]<<<grid, block, 0, stream>>>(args);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pimc(bool chain_update, const PimcArgs &args, int grid, int block,
+                        cudaStream_t stream) {
+    if (chain_update)
+        pimc_kernel<true><<<grid, block, 0, stream>>>(args);
+    else
+        pimc_kernel<false><<<grid, block, 0, stream>>>(args);
     return cudaGetLastError();
 }
 

@@ -33,6 +33,8 @@ cudaError_t sd_occupancy(bool sparse, bool smem, int warps_per_cta, int region_b
                          int *ctas_per_sm);
 cudaError_t launch_rmc(bool random_order, int proposal, const RmcArgs &args, int grid,
                        int block, cudaStream_t stream);
+cudaError_t launch_pimc(bool chain_update, const PimcArgs &args, int grid, int block,
+                        cudaStream_t stream);
 cudaError_t acceptance_check(int64_t samples, uint64_t seed, unsigned long long *d_counts);
 
 }  // namespace b200sa

@@ -140,6 +140,45 @@ struct RmcArgs {
     unsigned long long *near;
 };
 
+// Arguments of the path-integral Monte Carlo kernel (pimc_kernel.cuh).  One
+// thread per sample (a "slot"); every slot owns an mt19937 state and a
+// scratch area in global memory.  Break lists have a fixed capacity per
+// variable; proposals and domains per update have one too.
+struct PimcArgs {
+    int32_t n;
+    int64_t m;
+    const uint2 *vinfo;      // [n] {list start, degree}
+    const int32_t *col;      // adjacency, coupler input order
+    const double *w;
+    const double *h;
+    const int32_t *cu, *cv;  // COO (energy order)
+    const double *cw;
+    const double *hp, *hd;   // [num_betas] problem (invTemp) and driver (Gamma) schedules
+    int32_t num_betas;
+    int32_t sweeps_per_beta;
+    double jchain;           // chain coupling (Swendsen-Wang joins)
+    int32_t qpc;             // qubits per chain (chain update)
+    int32_t chains;          // n / qpc
+    const uint32_t *seeds;
+    int32_t shared_stream;   // 1: one thread, samples in order, one generator
+    int32_t num_samples;
+    int8_t *states;          // [num_samples][n], the first Trotter slice
+    int32_t *counts;         // [num_samples][n] breaks per variable
+    int32_t *breaks;         // [num_samples][n][cap_breaks]
+    int32_t cap_breaks;
+    int32_t cap_props;       // proposals per qubit and update
+    uint32_t *mt;            // [slots][kMtWords]
+    int32_t *scratch_i;      // [slots][scratch_ints]
+    double *scratch_d;       // [slots][scratch_doubles]
+    int64_t scratch_ints, scratch_doubles;
+    double *energies;
+    int8_t *stats;           // [num_samples][points][n], or null
+    int32_t interval;
+    unsigned long long *near;
+    int32_t *overflow;       // set when a capacity would be exceeded
+};
+constexpr int kMtWords = 624;
+
 // Nibble tables of the RNG jump matrix: entry [k][v] is the jump applied to
 // the state whose only set bits are the nibble value v at nibble position k.
 constexpr int kJumpNibbles = 32;

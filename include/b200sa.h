@@ -46,6 +46,7 @@ extern "C" {
 #define B200SA_ENOMEM (-3)   /* host or device allocation failed */
 #define B200SA_ENODEV (-4)   /* no usable sm_100 device */
 #define B200SA_ETIMEOUT (-5) /* a bounded device wait expired */
+#define B200SA_ERANGE (-6)   /* a fixed capacity was exceeded (call again with more) */
 
 /* cpu_sa.h:36-39 */
 #define B200SA_GIBBS 0
@@ -246,6 +247,45 @@ B200SA_API int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
                                    uint8_t *statistics, int32_t schedule_sample_interval,
                                    int32_t device, int64_t *near_ties, char *err,
                                    size_t errlen);
+
+/* ---- Path-integral Monte Carlo annealing (SQA) ----------------------------
+ * Replaces general_simulated_annealing of localPIMC
+ * (dwave/samplers/sqa/src/localPIMC.cpp:585-715, localPIMC.h:55-81; bound at
+ * dwave/samplers/sqa/pimc_annealing.pyx:45-283).  A sample is a set of world
+ * lines over 2^16 Trotter slices: the first slice (states, int8 +-1, host,
+ * num_samples x num_vars, overwritten) and, per variable, the slices where
+ * its spin flips (its breaks).  hp_field / hd_field: num_betas inverse
+ * temperatures (invTemp) and transverse fields (Gamma); every schedule step
+ * makes sweeps_per_beta * num_vars updates of uniformly drawn qubits
+ * (qubits_per_update == 1) or of chains of qubits_per_chain consecutive
+ * variables (any other value; Swendsen-Wang joins with
+ * chain_coupler_strength).  seeds: num_seeds == 1 continues one mt19937 stream
+ * over the samples exactly as one reference call; num_seeds == num_samples
+ * makes sample r equal a reference call with num_samples = 1 and seed =
+ * seeds[r] (samples run in parallel).  A seed of 0 (the reference's
+ * nondeterministic generator) draws a nonzero seed from std::random_device.
+ * project_inputs == 0: sample r starts from num_breaks[r][v] positions per
+ * variable read in order from breaks_in (breaks_in_size entries).
+ * project_outputs == 0: num_breaks receives the final counts and breaks_out
+ * (breaks_out_size entries) the positions, filled as the reference's
+ * readBreaks fills its buffer (localPIMC.cpp:185-200).  statistics receives,
+ * for schedule_sample_interval > 0, the first slice after every schedule
+ * index divisible by the interval (num_samples x points x num_vars, points =
+ * 1 + (num_betas - 1) / interval).  break_capacity bounds the breaks of a
+ * variable and the proposals of one update (0: from the largest Gamma);
+ * exceeding it returns B200SA_ERANGE.  near_ties (optional) counts log / tanh
+ * / exp decisions within 2^-48 of their threshold (expected 0).  Returns
+ * num_samples or a negative error. */
+B200SA_API int b200sa_path_anneal(
+    int32_t num_vars, const double *h, int64_t num_couplers, const int32_t *coupler_starts,
+    const int32_t *coupler_ends, const double *coupler_weights, int32_t num_samples,
+    int8_t *states, double *energies, int32_t sweeps_per_beta, int32_t num_betas,
+    const double *hp_field, const double *hd_field, double chain_coupler_strength,
+    int32_t qubits_per_chain, int32_t qubits_per_update, const uint32_t *seeds,
+    int32_t num_seeds, int32_t project_inputs, int32_t project_outputs, int32_t *num_breaks,
+    const int32_t *breaks_in, int64_t breaks_in_size, int32_t *breaks_out,
+    int64_t breaks_out_size, int8_t *statistics, int32_t schedule_sample_interval,
+    int32_t break_capacity, int32_t device, int64_t *near_ties, char *err, size_t errlen);
 
 /* ---- Sample moments (no reference counterpart) ------------------------------
  * For the gradient of log Z of p(s) ~ exp(-beta*E(s)), E as in cpu_sa.cpp:210-227:

@@ -1,8 +1,9 @@
-"""Generate golden vectors from the reference's own simulated-annealing and
-steepest-descent code.
+"""Generate golden vectors from the reference's own simulated-annealing,
+steepest-descent and SQA (rotor and path-integral) code.
 
     bash oracle/build_ref.sh            # reference extensions from their sources
-    python tests/golden/make_golden.py  # writes tests/golden/*.npz, tests/golden/descent/*.npz
+    python tests/golden/make_golden.py  # writes tests/golden/*.npz and the
+                                        # descent/, rotor/ and pimc/ subfolders
 
 Each fixture stores the inputs and the reference's outputs.  Per-read
 fixtures hold, for each read r, the result of one reference call with
@@ -285,6 +286,101 @@ def main_rotor():
         print(f"rotor/{name}: samples={s0.shape[0]} n={len(c['h'])}")
 
 
+def pimc_cases():
+    """Path-integral (SQA) fixtures: single-qubit and chain updates, per-sample
+    calls and continued-stream calls, statistics, final break positions (with
+    a buffer too small for all of them in one case), quantum initial states,
+    no transverse field, self-loops and repeated couplers."""
+    rng = np.random.default_rng(20240715)
+    out = {}
+
+    def problem(n, p, extra=()):
+        pairs = [(a, b) for a in range(n) for b in range(a + 1, n) if rng.random() < p]
+        pairs += list(extra)
+        return dict(h=rng.normal(0, 0.4, n), u=np.array([q[0] for q in pairs], np.int32),
+                    v=np.array([q[1] for q in pairs], np.int32), J=rng.normal(0, 1, len(pairs)))
+
+    def case(name, prob, R, hp, hd, spb=2, qpc=1, qpu=1, jchain=1.0, shared=False, interval=0,
+             proj_in=True, proj_out=False, out_size=1 << 16):
+        n = len(prob["h"])
+        c = dict(prob, states0=states(rng, R, n), spb=spb, hp=np.asarray(hp, np.float64),
+                 hd=np.asarray(hd, np.float64), qpc=qpc, qpu=qpu, jchain=jchain,
+                 seed=int(rng.integers(1, 2**31)), shared=shared, interval=interval,
+                 proj_in=proj_in, proj_out=proj_out, out_size=out_size)
+        nb = np.zeros((R, n), np.intc)
+        bin_ = np.zeros(1, np.intc)
+        if not proj_in:  # n increasing positions per variable
+            nb[:] = n
+            bin_ = np.concatenate([np.sort(rng.choice(65536, n, replace=False))
+                                   for _ in range(R * n)]).astype(np.intc)
+        c.update(num_breaks0=nb, breaks_in=bin_)
+        out[name] = c
+
+    p24 = problem(24, 0.2)
+    ramp = (np.geomspace(0.1, 3.0, 12), np.geomspace(4.0, 0.05, 12))
+    case("qubit_per_read", p24, 6, *ramp, interval=3)
+    case("qubit_shared", p24, 5, *ramp, shared=True, interval=4)
+    case("qubit_high_field", p24, 5, np.full(6, 0.7), np.full(6, 8.0))
+    case("qubit_no_field", p24, 5, np.geomspace(0.2, 4.0, 8), np.zeros(8), proj_out=True)
+    case("qubit_small_buffer", p24, 4, np.full(5, 0.8), np.full(5, 6.0), shared=True,
+         out_size=300)
+    p16 = problem(16, 0.2)
+    case("chain4_per_read", p16, 5, np.geomspace(0.2, 2.0, 8), np.full(8, 5.0), qpc=4, qpu=4,
+         jchain=-1.8)
+    case("chain2_shared", p16, 4, *ramp, qpc=2, qpu=2, jchain=-3.0, shared=True, interval=2)
+    p18 = problem(18, 0.2)
+    case("chain3_per_read", p18, 4, np.full(6, 0.5), np.full(6, 12.0), qpc=3, qpu=3,
+         jchain=-0.4)
+    p8 = problem(8, 0.3)
+    case("quantum_inputs", p8, 3, np.geomspace(0.2, 2.0, 5), np.full(5, 2.0), proj_in=False)
+    loops = problem(10, 0.25, extra=[(2, 2), (3, 7), (3, 7), (7, 3)])
+    case("self_loops_repeats", loops, 4, np.full(6, 1.0), np.full(6, 3.0))
+    return out
+
+
+def main_pimc():
+    mod = oracle.reference_pimc_module()
+    if mod is None:
+        raise SystemExit("build the reference first: bash oracle/build_ref.sh")
+    outdir = os.path.join(HERE, "pimc")
+    os.makedirs(outdir, exist_ok=True)
+    for name, c in pimc_cases().items():
+        s0 = c["states0"]
+        R, n = s0.shape
+        args = (list(map(float, c["h"])), list(map(int, c["u"])), list(map(int, c["v"])),
+                list(map(float, c["J"])), c["spb"], c["hp"], c["hd"], 1.0, c["jchain"],
+                c["qpc"], c["qpu"])
+        if c["shared"]:
+            bo = np.zeros(c["out_size"], np.intc)
+            s, e, st, nb, bo = mod.simulated_annealing(
+                R, *args, c["seed"], s0.copy(), c["proj_in"], c["proj_out"],
+                c["num_breaks0"].copy(), c["breaks_in"].copy(), bo, c["interval"])
+            s, e, st, nb = map(np.asarray, (s, e, st, nb))
+        else:
+            outs, bufs = [], []
+            per = n * n if not c["proj_in"] else 0
+            for r in range(R):
+                bo = np.zeros(c["out_size"], np.intc)
+                bin_r = c["breaks_in"][r * per:(r + 1) * per] if per else c["breaks_in"]
+                o = mod.simulated_annealing(
+                    1, *args, c["seed"] + r, s0[r:r + 1].copy(), c["proj_in"], c["proj_out"],
+                    c["num_breaks0"][r:r + 1].copy(), np.ascontiguousarray(bin_r), bo,
+                    c["interval"])
+                outs.append(o)
+                bufs.append(np.asarray(o[4])[:int(np.asarray(o[3]).sum())])
+            s = np.concatenate([np.asarray(o[0]) for o in outs])
+            e = np.concatenate([np.asarray(o[1]) for o in outs])
+            st = np.concatenate([np.asarray(o[2]) for o in outs])
+            nb = np.concatenate([np.asarray(o[3]) for o in outs])
+            bo = np.zeros(c["out_size"], np.intc)
+            flat = np.concatenate(bufs) if bufs else np.zeros(0, np.intc)
+            bo[:len(flat)] = flat
+        np.savez_compressed(os.path.join(outdir, f"{name}.npz"), **c, out_states=s.astype(np.int8),
+                            out_energies=e.astype(np.float64), out_stats=st.astype(np.int8),
+                            out_num_breaks=nb.astype(np.intc), out_breaks=np.asarray(bo, np.intc))
+        print(f"pimc/{name}: samples={R} n={n} breaks={int(nb.sum()) if not c['proj_out'] else '-'}")
+
+
 def main():
     if oracle.reference_module() is None:
         raise SystemExit("build the reference first: bash oracle/build_ref.sh")
@@ -306,3 +402,4 @@ if __name__ == "__main__":
     main()
     main_descent()
     main_rotor()
+    main_pimc()
