@@ -72,10 +72,12 @@ def parse_args():
                     help="timed Boltzmann-machine gradient steps (after one untimed step)")
     ap.add_argument("--bm-target-reads", type=int, default=1024,
                     help="reads behind the BM target correlations (outside the timed steps)")
-    ap.add_argument("--descent-samples", type=int, default=4096,
+    ap.add_argument("--descent-samples", type=int, default=16384,
                     help="steepest-descent leg: samples (0 skips it)")
-    ap.add_argument("--rotor-samples", type=int, default=4096,
+    ap.add_argument("--rotor-samples", type=int, default=32768,
                     help="rotor-model (SQA) annealing leg: samples (0 skips it)")
+    ap.add_argument("--pimc-samples", type=int, default=16384,
+                    help="path-integral (SQA) annealing leg: samples (0 skips it)")
     return ap.parse_args()
 
 
@@ -415,6 +417,64 @@ def bench_rotor(args, local, world, rank):
     return out
 
 
+def bench_pimc(args, local, world, rank):
+    """Path-integral Monte Carlo (SQA) annealing (b200sa_path_anneal, host
+    buffers, single-qubit updates, per-sample seeds) on a random 6-regular
+    problem, n = 512, J~N(0,1), h~N(0,0.1), 16 schedule steps of one sweep
+    (invTemp 0.1 -> 5, transverse field 5 -> 0.05, geometric), uniform random
+    initial states; one untimed call, then two timed calls.  Rank 0 also times
+    the reference's own extension (one call per sample, seed + r) on all host
+    threads over a bounded sample."""
+    import oracle
+    from b200sa.sqa import path_annealing
+    rng = np.random.default_rng(31)
+    n, u, v = workloads.random_regular(512, 6, rng, graph_seed=31)
+    J = rng.normal(0, 1, u.shape[0])
+    h = rng.normal(0, 0.1, n)
+    hp = np.geomspace(0.1, 5.0, 16)
+    hd = np.geomspace(5.0, 0.05, 16)
+    R = args.pimc_samples
+    init = (2 * rng.integers(0, 2, (R, n)) - 1).astype(np.int8)
+    nb = np.zeros((R, n), np.intc)
+    none = np.zeros(1, np.intc)
+    call = lambda st: path_annealing(R, h, u, v, J, 1, hp, hd, 1.0, 1.0, 1, 1, 4321, st, True,
+                                     True, nb, none, none, 0, device=local)
+    call(init.copy())
+    times = []
+    for _ in range(2):
+        st = init.copy()
+        t0 = time.perf_counter()
+        call(st)
+        times.append(max_over_ranks(time.perf_counter() - t0, world, "cuda"))
+    sec = statistics.median(times)
+    updates = R * n * len(hp)
+    out = {"workload": "path-integral annealing, random 6-regular n=512, J~N(0,1), h~N(0,0.1), "
+                       "16 steps x 1 sweep, invTemp 0.1->5, Gamma 5->0.05, single-qubit updates",
+           "samples": R, "updates_per_s": world * updates / sec, "seconds": sec,
+           "note": "host buffers in and out (the call as a user makes it)"}
+    ref = oracle.reference_pimc_module() if (rank == 0 and not args.no_cpu) else None
+    if ref is not None:
+        from concurrent.futures import ThreadPoolExecutor
+        threads = cpu_threads()
+        sample = min(R, threads * 32)
+        args_ref = (list(map(float, h)), list(map(int, u)), list(map(int, v)),
+                    list(map(float, J)), 1, hp, hd, 1.0, 1.0, 1, 1)
+
+        def one(r):  # one call per sample, seed + r; the binding releases the GIL
+            ref.simulated_annealing(1, *args_ref, 4321 + r, init[r:r + 1].copy(), True, True,
+                                    np.zeros((1, n), np.intc), np.zeros(1, np.intc),
+                                    np.zeros(1, np.intc), 0)
+
+        with ThreadPoolExecutor(threads) as ex:
+            t0 = time.perf_counter()
+            list(ex.map(one, range(sample)))
+            cpu = time.perf_counter() - t0
+        out["cpu_reference"] = {"updates_per_s": sample * n * len(hp) / cpu, "cores": threads,
+                                "sample": f"{sample} of the same samples"}
+        out["gpu_over_cpu"] = out["updates_per_s"] / out["cpu_reference"]["updates_per_s"]
+    return out
+
+
 def bench_bm(args, local, world):
     """Batched Boltzmann-machine learning: 64 six-regular models, n~U[256,2048],
     ground truth J*~N(0,0.5), h*=0; per gradient step 1024 fixed-beta (beta=1)
@@ -604,6 +664,8 @@ def run_ours(args):
         line["descent"] = bench_descent(args, local, world, rank)
     if args.rotor_samples > 0:
         line["rotor"] = bench_rotor(args, local, world, rank)
+    if getattr(args, "pimc_samples", 0) > 0:
+        line["pimc"] = bench_pimc(args, local, world, rank)
 
     if rank == 0 and not args.no_cpu:
         cb = cpu_sample(probs, args.cpu_budget)

@@ -151,7 +151,10 @@ extern "C" int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
     a.cos_table = dtab.ptr;
     a.sin_table = dtab.ptr + 256;
     a.near = dnear.ptr;
-    const int block = 128;
+    // Each read is one latency-bound chain: small CTAs spread the reads over
+    // every SM (up to 32 CTAs per SM); 64-thread CTAs once the reads fill them.
+    const int sms = prop.multiProcessorCount;
+    const int block = R >= (size_t)sms * 32 * 64 ? 64 : 32;
     const int grid = shared ? 1 : (int)((R + block - 1) / block);
     B200SA_CUDA(launch_rmc(randomize_order != 0, proposal, a, grid, block, nullptr));
     B200SA_CUDA(cudaDeviceSynchronize());

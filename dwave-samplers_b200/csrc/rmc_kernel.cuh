@@ -32,7 +32,7 @@ __device__ __forceinline__ bool rmc_metropolis(double x, uint64_t r, unsigned &n
 }
 
 template <bool RANDOM_ORDER, int PROPOSAL>
-__global__ void __launch_bounds__(256) rmc_kernel(RmcArgs A) {
+__global__ void __launch_bounds__(64) rmc_kernel(RmcArgs A) {
     __shared__ double cs[256], sn[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
         cs[i] = A.cos_table[i];
