@@ -32,21 +32,16 @@ namespace b200sa {
 
 constexpr int kPimcSlices = 65536;  // numTrotterSlices, localPIMC.h:88
 
-// mt19937 regeneration of all 624 words (Matsumoto & Nishimura 1998), in the
-// three ranges where word i + 397 is still old, already new, and the last word.
-__device__ __noinline__ void pimc_mt_twist(uint32_t *mt) {
-    auto mix = [](uint32_t a, uint32_t b, uint32_t c) {
-        const uint32_t y = (a & 0x80000000u) | (b & 0x7fffffffu);
-        return c ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
-    };
-    for (int i = 0; i < 227; ++i) mt[i] = mix(mt[i], mt[i + 1], mt[i + 397]);
-    for (int i = 227; i < 623; ++i) mt[i] = mix(mt[i], mt[i + 1], mt[i - 227]);
-    mt[623] = mix(mt[623], mt[0], mt[396]);
-}
-
+// mt19937 (Matsumoto & Nishimura 1998), regenerated one word per draw: word
+// i is replaced by its successor from words i, i + 1 and i + 397 (mod 624) just
+// before it is output.  Regenerating in index order is what the block
+// regeneration of all 624 words does, so the stream is the same; the cost is
+// the same for every draw, so threads of a warp never wait on one thread's
+// 624-word burst.
 struct PimcRng {
     uint32_t *mt;
-    int idx;
+    int idx;       // next word to regenerate and output
+    uint32_t cur;  // mt[idx], not yet regenerated
 
     __device__ void seed(uint32_t s) {
         uint32_t x = s;
@@ -55,14 +50,18 @@ struct PimcRng {
             x = 1812433253u * (x ^ (x >> 30)) + (uint32_t)i;
             mt[i] = x;
         }
-        idx = kMtWords;
+        idx = 0;
+        cur = s;
     }
     __device__ __forceinline__ uint32_t next() {
-        if (idx >= kMtWords) {
-            pimc_mt_twist(mt);
-            idx = 0;
-        }
-        uint32_t y = mt[idx++];
+        const int i1 = idx == kMtWords - 1 ? 0 : idx + 1;
+        const int im = idx < kMtWords - 397 ? idx + 397 : idx - (kMtWords - 397);
+        const uint32_t b = mt[i1];
+        const uint32_t t = (cur & 0x80000000u) | (b & 0x7fffffffu);
+        uint32_t y = mt[im] ^ (t >> 1) ^ ((t & 1u) ? 0x9908b0dfu : 0u);
+        mt[idx] = y;
+        idx = i1;
+        cur = b;
         y ^= y >> 11;
         y ^= (y << 7) & 0x9d2c5680u;
         y ^= (y << 15) & 0xefc60000u;
