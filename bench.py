@@ -76,7 +76,7 @@ def parse_args():
                     help="steepest-descent leg: samples (0 skips it)")
     ap.add_argument("--rotor-samples", type=int, default=32768,
                     help="rotor-model (SQA) annealing leg: samples (0 skips it)")
-    ap.add_argument("--pimc-samples", type=int, default=16384,
+    ap.add_argument("--pimc-samples", type=int, default=65536,
                     help="path-integral (SQA) annealing leg: samples (0 skips it)")
     return ap.parse_args()
 
