@@ -79,15 +79,11 @@ extern "C" int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
     DevArray<int32_t> dcol, dcu, dcv;
     DevArray<double> dw, dh, dtf, dcw, dhp, dhd, dde, den, dtab;
     DevArray<uint64_t> dseeds;
-    DevArray<uint8_t> dst, dstats;
+    DevArray<uint8_t> dst, drows, dstats;
     DevArray<unsigned long long> dnear;
     std::vector<uint2> vinfo(n);
     for (size_t v = 0; v < n; ++v)
         vinfo[v] = make_uint2(adj.vinfo[2 * v], adj.vinfo[2 * v + 1] & kDegMask);
-    // Interleaved states: element (v, r) at v * R + r.
-    std::vector<uint8_t> inter(n * R);
-    for (size_t r = 0; r < R; ++r)
-        for (size_t v = 0; v < n; ++v) inter[v * R + r] = states[r * n + v];
     std::vector<double> tab(512);
     std::copy(cos_t, cos_t + 256, tab.begin());
     std::copy(sin_t, sin_t + 256, tab.begin() + 256);
@@ -104,6 +100,7 @@ extern "C" int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
     B200SA_CUDA(dtab.alloc(512));
     B200SA_CUDA(dseeds.alloc((size_t)num_seeds));
     B200SA_CUDA(dst.alloc(n * R));
+    B200SA_CUDA(drows.alloc(n * R));
     B200SA_CUDA(dde.alloc(n * R));
     B200SA_CUDA(den.alloc(R));
     B200SA_CUDA(dnear.alloc(1));
@@ -123,7 +120,7 @@ extern "C" int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
     B200SA_CUDA(up(dhd.ptr, hd_field, 8 * (size_t)num_betas));
     B200SA_CUDA(up(dtab.ptr, tab.data(), 8 * 512));
     B200SA_CUDA(up(dseeds.ptr, seeds, 8 * (size_t)num_seeds));
-    B200SA_CUDA(up(dst.ptr, inter.data(), n * R));
+    B200SA_CUDA(up(drows.ptr, states, n * R));
     B200SA_CUDA(cudaMemset(dnear.ptr, 0, sizeof(unsigned long long)));
     RmcArgs a{};
     a.n = num_vars;
@@ -143,6 +140,7 @@ extern "C" int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
     a.seeds = dseeds.ptr;
     a.shared_stream = shared ? 1 : 0;
     a.num_samples = num_samples;
+    a.rows = drows.ptr;
     a.states = dst.ptr;
     a.de = dde.ptr;
     a.energies = den.ptr;
@@ -158,9 +156,7 @@ extern "C" int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
     const int grid = shared ? 1 : (int)((R + block - 1) / block);
     B200SA_CUDA(launch_rmc(randomize_order != 0, proposal, a, grid, block, nullptr));
     B200SA_CUDA(cudaDeviceSynchronize());
-    B200SA_CUDA(cudaMemcpy(inter.data(), dst.ptr, n * R, cudaMemcpyDeviceToHost));
-    for (size_t r = 0; r < R; ++r)
-        for (size_t v = 0; v < n; ++v) states[r * n + v] = inter[v * R + r];
+    B200SA_CUDA(cudaMemcpy(states, drows.ptr, n * R, cudaMemcpyDeviceToHost));
     B200SA_CUDA(cudaMemcpy(energies, den.ptr, 8 * R, cudaMemcpyDeviceToHost));
     unsigned long long near = 0;
     B200SA_CUDA(cudaMemcpy(&near, dnear.ptr, sizeof(near), cudaMemcpyDeviceToHost));

@@ -7,7 +7,9 @@
 // number of random numbers, so a read is one sequential chain; many reads run
 // side by side instead.  States and delta energies are interleaved across
 // reads (element (v, r) at v * R + r), so in sequential order the 32 reads of
-// a warp touch one variable in one transaction.
+// a warp touch one variable in one transaction.  Each thread copies its
+// sample's row of the caller's row-major states into that layout first and
+// back at the end.
 //
 // Arithmetic follows cpu_rotormc.cpp operation for operation:
 //   local field (:46-60)       h + cos(theta_nb) * J, adjacency order
@@ -56,6 +58,8 @@ __global__ void __launch_bounds__(64) rmc_kernel(RmcArgs A) {
         const int64_t R64 = R;
         uint8_t *st = A.states + r;  // element v at st[v * R]
         double *de = A.de + r;
+        uint8_t *row = A.rows + (int64_t)r * n;
+        for (int v = 0; v < n; ++v) st[v * R64] = row[v];
         auto field = [&](int var) {
             const uint2 vi = __ldg(&A.vinfo[var]);
             double e = __ldg(&A.h[var]);
@@ -153,6 +157,7 @@ __global__ void __launch_bounds__(64) rmc_kernel(RmcArgs A) {
             e = __dadd_rn(e, __dmul_rn(__dmul_rn(cs[st[(int64_t)__ldg(&A.cu[c]) * R64]], __ldg(&A.cw[c])),
                                        cs[st[(int64_t)__ldg(&A.cv[c]) * R64]]));
         A.energies[r] = e;
+        for (int v = 0; v < n; ++v) row[v] = st[v * R64];
     }
     if (near) atomicAdd(A.near, (unsigned long long)near);
 }

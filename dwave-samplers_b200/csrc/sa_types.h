@@ -131,7 +131,8 @@ struct RmcArgs {
     const uint64_t *seeds;
     int32_t shared_stream;   // 1: one thread, samples in order, one RNG stream
     int32_t num_samples;
-    uint8_t *states;         // interleaved: element (v, r) at v * num_samples + r
+    uint8_t *rows;           // [num_samples][n] initial states in, final states out
+    uint8_t *states;         // working copy, interleaved: element (v, r) at v * num_samples + r
     double *de;              // interleaved like states
     double *energies;
     uint8_t *stats;          // [num_samples][points][n], or null
