@@ -27,7 +27,7 @@ def test_golden_fixtures(name):
     np.testing.assert_array_equal(k, c["out_steps"])
 
 
-@pytest.mark.parametrize("n", [1, 5, 33, 257, 1500, 9000])
+@pytest.mark.parametrize("n", [1, 5, 33, 257, 1500, 4096, 9000])
 @pytest.mark.parametrize("mode", [False, True])
 def test_random_problems_vs_oracle(n, mode):
     rng = np.random.default_rng(n + 7 * mode)
