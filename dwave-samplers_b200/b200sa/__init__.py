@@ -8,8 +8,8 @@ Public surface:
   launch (graph replay, in-place weights, autotuning).
 * :mod:`b200sa.sampler` -- ``SimulatedAnnealingSampler`` front end (dimod-free).
 * :mod:`b200sa.greedy` -- steepest descent (``dwave.samplers.greedy``).
-* :mod:`b200sa.sqa` -- rotor-model annealing (``dwave.samplers.sqa``'s rotor
-  Monte Carlo binding).
+* :mod:`b200sa.sqa` -- ``dwave.samplers.sqa``'s two bindings: rotor-model
+  annealing and path-integral Monte Carlo annealing.
 * :mod:`b200sa.autograd`, :mod:`b200sa.bm` -- differentiable fixed-beta
   sampling and batched Boltzmann-machine learning.
 """
@@ -17,4 +17,4 @@ from .simulated_annealing import per_read_seeds, simulated_annealing
 from .batch import Plan, sample_batch
 
 __all__ = ["simulated_annealing", "per_read_seeds", "sample_batch", "Plan"]
-__version__ = "0.4.0"
+__version__ = "0.5.0"
