@@ -9,7 +9,8 @@ Public surface:
 * :mod:`b200sa.sampler` -- ``SimulatedAnnealingSampler`` front end (dimod-free).
 * :mod:`b200sa.greedy` -- steepest descent (``dwave.samplers.greedy``).
 * :mod:`b200sa.sqa` -- ``dwave.samplers.sqa``'s two bindings: rotor-model
-  annealing and path-integral Monte Carlo annealing.
+  annealing and path-integral Monte Carlo annealing; :mod:`b200sa.sqa_sampler`
+  -- its two sampler classes (dimod-free).
 * :mod:`b200sa.autograd`, :mod:`b200sa.bm` -- differentiable fixed-beta
   sampling and batched Boltzmann-machine learning.
 """
