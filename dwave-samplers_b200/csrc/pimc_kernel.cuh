@@ -193,6 +193,33 @@ __device__ void pimc_add_j(double *eff, const int32_t *lab, const int32_t *itf, 
     }
 }
 
+// Adds h and every neighbour's world line of qubit q to the domain fields,
+// neighbours in adjacency order.  The spin, break count and coupling of up
+// to four neighbours are loaded before any field is written, so those loads
+// overlap instead of waiting behind the previous neighbour's stores.
+__device__ void pimc_fields(const PimcArgs &A, const PimcWorld &W, int q, double *eff,
+                            const int32_t *lab, const int32_t *itf, int nd) {
+    pimc_add_h(eff, lab, itf, nd, __ldg(&A.h[q]));
+    const uint2 vi = __ldg(&A.vinfo[q]);
+    const unsigned end = vi.x + vi.y;
+    for (unsigned k0 = vi.x; k0 < end; k0 += 4) {
+        int nb[4], cnt[4];
+        double js[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) nb[j] = k0 + j < end ? __ldg(&A.col[k0 + j]) : 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (k0 + j < end) {
+                cnt[j] = W.cnt[nb[j]];
+                js[j] = __dmul_rn((double)W.s[nb[j]], __ldg(&A.w[k0 + j]));
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (k0 + j < end) pimc_add_j(eff, lab, itf, nd, W.list(nb[j]), cnt[j], js[j]);
+    }
+}
+
 __device__ __forceinline__ int pimc_gibbs(PimcRng &g, PimcWorld &W, double field) {
     const double thr = __dadd_rn(__dmul_rn(g.canonical(), 2.0), -1.0);  // uniform(-1, 1)
     const double t = tanh(__dmul_rn(W.beta, field));
@@ -240,13 +267,7 @@ __device__ void pimc_qubit_update(const PimcArgs &A, PimcRng &g, PimcWorld &W, i
     const int nd = pimc_interfaces(g, W, sp, props, A.cap_props, itf);
     if (W.overflow) return;
     for (int i = 0; i < nd; ++i) eff[i] = 0.0;
-    pimc_add_h(eff, nullptr, itf, nd, __ldg(&A.h[sp]));
-    const uint2 vi = __ldg(&A.vinfo[sp]);
-    for (unsigned k = vi.x; k < vi.x + vi.y; ++k) {
-        const int nb = __ldg(&A.col[k]);
-        pimc_add_j(eff, nullptr, itf, nd, W.list(nb), W.cnt[nb],
-                   __dmul_rn((double)W.s[nb], __ldg(&A.w[k])));
-    }
+    pimc_fields(A, W, sp, eff, nullptr, itf, nd);
     for (int d = 0; d < nd; ++d) sv[d] = pimc_gibbs(g, W, eff[d]);
     if (!pimc_store(W, sp, itf, nd, [&](int d) { return sv[d]; })) W.overflow = true;
 }
@@ -337,15 +358,7 @@ __device__ void pimc_chain_update(const PimcArgs &A, PimcRng &g, PimcWorld &W, i
     }
     for (int k = 0; k < ncomp; ++k) eff[k] = 0.0;
     for (int c = 0; c < Q; ++c) {
-        const int q = Q * sp + c;
-        const int nd = off[c + 1] - off[c];
-        pimc_add_h(eff, lab + off[c], itf + c * C, nd, __ldg(&A.h[q]));
-        const uint2 vi = __ldg(&A.vinfo[q]);
-        for (unsigned k = vi.x; k < vi.x + vi.y; ++k) {
-            const int nb = __ldg(&A.col[k]);
-            pimc_add_j(eff, lab + off[c], itf + c * C, nd, W.list(nb), W.cnt[nb],
-                       __dmul_rn((double)W.s[nb], __ldg(&A.w[k])));
-        }
+        pimc_fields(A, W, Q * sp + c, eff, lab + off[c], itf + c * C, off[c + 1] - off[c]);
     }
     for (int k = 0; k < ncomp; ++k) sv[k] = pimc_gibbs(g, W, eff[k]);
     for (int c = 0; c < Q; ++c) {
