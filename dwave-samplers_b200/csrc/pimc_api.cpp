@@ -111,7 +111,11 @@ extern "C" int b200sa_path_anneal(
             do s = rd(); while (s == 0);
         }
     }
-    const int points = schedule_sample_interval ? 1 + (num_betas - 1) / schedule_sample_interval : 0;
+    // Schedule indices divisible by the interval; none for an empty schedule
+    // (the bindings' floor division gives 0 there too).
+    const int points = schedule_sample_interval && num_betas > 0
+                           ? 1 + (num_betas - 1) / schedule_sample_interval
+                           : 0;
 
     b200sa_problem q{};
     q.num_vars = num_vars;

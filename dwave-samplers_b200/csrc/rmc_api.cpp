@@ -73,7 +73,11 @@ extern "C" int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
     int rc = select_device(device, prop, err, errlen);
     if (rc) return rc;
     const bool shared = num_seeds == 1 && num_samples > 1;
-    const int points = schedule_sample_interval ? 1 + (num_betas - 1) / schedule_sample_interval : 0;
+    // Schedule indices divisible by the interval; none for an empty schedule
+    // (the bindings' floor division gives 0 there too).
+    const int points = schedule_sample_interval && num_betas > 0
+                           ? 1 + (num_betas - 1) / schedule_sample_interval
+                           : 0;
     const size_t n = (size_t)num_vars, R = (size_t)num_samples, m = (size_t)num_couplers;
     DevArray<uint2> dvinfo;
     DevArray<int32_t> dcol, dcu, dcv;

@@ -118,3 +118,16 @@ def test_interrupt_cuts_after_first_true():
                          np.zeros((R, n), np.intc), np.zeros(1, np.intc), np.zeros(1, np.intc),
                          0, stop)
     assert len(out[0]) == 2 and len(out[1]) == 2 and len(calls) == 2
+
+
+def test_empty_schedule_with_statistics():
+    # No schedule steps: nothing is sampled, the statistics have no points and
+    # the states come back unchanged.
+    R, n = 4, 6
+    st0 = np.ones((R, n), np.int8)
+    s, e, st, nb, bo = path_annealing(R, [0.1] * n, [0, 1], [1, 2], [1.0, -1.0], 1, [], [], 1.0,
+                                      1.0, 1, 1, 5, st0.copy(), True, True,
+                                      np.zeros((R, n), np.intc), np.zeros(1, np.intc),
+                                      np.zeros(1, np.intc), 1)
+    assert st.shape == (R, 0, n)
+    np.testing.assert_array_equal(s, st0)

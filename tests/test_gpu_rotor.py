@@ -61,3 +61,13 @@ def test_interrupt_cuts_after_first_true():
                                    [1.0, 2.0], [1.0, 0.5], 5, st0, False, "MetropolisUniform",
                                    0, stop)
     assert len(s) == 3 and len(e) == 3 and len(calls) == 3
+
+
+def test_empty_schedule_with_statistics():
+    # No schedule steps: nothing is sampled and the statistics have no points.
+    R, n = 4, 6
+    st0 = np.full((R, n), 7, np.uint8)
+    s, e, st = simulated_annealing(R, [0.1] * n, [0, 1], [1, 2], [1.0, -1.0], [1.0] * n, 1, [],
+                                   [], 5, st0.copy(), False, "MetropolisUniform", 1)
+    assert st.shape == (R, 0, n)
+    np.testing.assert_array_equal(s, st0)
