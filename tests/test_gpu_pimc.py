@@ -131,3 +131,34 @@ def test_empty_schedule_with_statistics():
                                       np.zeros(1, np.intc), 1)
     assert st.shape == (R, 0, n)
     np.testing.assert_array_equal(s, st0)
+
+
+def test_chain_updates_from_quantum_states_vs_oracle():
+    # Chains of 4 starting from world lines with breaks (2 per variable), final
+    # breaks returned, per-sample seeds; the oracle runs one call per sample.
+    rng = np.random.default_rng(41)
+    R, n, q = 24, 48, 4
+    u = rng.integers(0, n, 120).astype(np.int32)
+    v = rng.integers(0, n, 120).astype(np.int32)
+    J, h = rng.normal(0, 1, 120), rng.normal(0, 0.3, n)
+    st0 = (2 * rng.integers(0, 2, (R, n)) - 1).astype(np.int8)
+    nb0 = np.full((R, n), 2, np.intc)
+    bin_ = np.sort(rng.choice(65536, size=(R * n, 2), replace=False), axis=1).astype(np.intc)
+    hp, hd = np.geomspace(0.2, 2.0, 6), np.full(6, 3.0)
+    s, e, _, nb, bo = path_annealing(R, h, u, v, J, 2, hp, hd, 1.0, -1.2, q, q, 77, st0.copy(),
+                                     False, False, nb0.copy(), bin_.ravel().copy(),
+                                     np.zeros(1 << 16, np.intc), 0)
+    ws, we, wnb, wl = [], [], [], []
+    for r in range(R):
+        o = oracle.pimc(h, u, v, J, st0[r:r + 1], 2, hp, hd, 77 + r, -1.2, q, q, False, False,
+                        num_breaks=nb0[r:r + 1], breaks_in=bin_[r * n:(r + 1) * n].ravel(),
+                        max_out=512)
+        ws.append(o[0])
+        we.append(o[1])
+        wnb.append(o[3])
+        wl.append(o[4])
+    wnb = np.concatenate(wnb)
+    np.testing.assert_array_equal(s, np.concatenate(ws))
+    np.testing.assert_array_equal(bits(e), bits(np.concatenate(we)))
+    np.testing.assert_array_equal(nb, wnb)
+    np.testing.assert_array_equal(bo, compose_breaks(wnb, np.concatenate(wl), len(bo)))
