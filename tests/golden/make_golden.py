@@ -335,6 +335,12 @@ def pimc_cases():
     case("quantum_inputs", p8, 3, np.geomspace(0.2, 2.0, 5), np.full(5, 2.0), proj_in=False)
     loops = problem(10, 0.25, extra=[(2, 2), (3, 7), (3, 7), (7, 3)])
     case("self_loops_repeats", loops, 4, np.full(6, 1.0), np.full(6, 3.0))
+    # Any qubits_per_update other than 1 updates whole chains of qubits_per_chain;
+    # with 1, chains are ignored.
+    case("chain3_update2", p18, 3, np.full(5, 0.6), np.full(5, 4.0), qpc=3, qpu=2,
+         jchain=-1.0)
+    case("qubit_ignores_chains", p16, 3, np.full(5, 0.6), np.full(5, 4.0), qpc=4, qpu=1,
+         jchain=-1.0)
     return out
 
 
@@ -375,6 +381,8 @@ def main_pimc():
             bo = np.zeros(c["out_size"], np.intc)
             flat = np.concatenate(bufs) if bufs else np.zeros(0, np.intc)
             bo[:len(flat)] = flat
+        if not c["interval"]:  # the binding returns an uninitialised array then
+            st = np.zeros_like(np.asarray(st))
         np.savez_compressed(os.path.join(outdir, f"{name}.npz"), **c, out_states=s.astype(np.int8),
                             out_energies=e.astype(np.float64), out_stats=st.astype(np.int8),
                             out_num_breaks=nb.astype(np.intc), out_breaks=np.asarray(bo, np.intc))

@@ -65,7 +65,7 @@ def oracle_run(c, max_out=512):
 
 
 def test_fixture_set():
-    assert len(PIMC) == 10
+    assert len(PIMC) == 12
 
 
 def test_mt19937_check_value():
