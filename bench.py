@@ -37,10 +37,6 @@ from b200sa import workloads  # noqa: E402
 METRIC = "spin-flip attempts/s, 1 B200: batched vs plain (bit-exact); BM grad steps/s"
 UNIT = "attempts/s"
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes (read + write) of one step's sweep launches on the full batch with
-# autotuned launches, from an ncu capture (metrics dram__bytes_read.sum and
-# dram__bytes_write.sum, one pass per launch): profiles/uneven_batch_step_dram_traffic.md.
-TRAFFIC_BYTES_PER_STEP = 2.019e13
 
 
 def parse_args():
@@ -78,6 +74,10 @@ def parse_args():
                     help="rotor-model (SQA) annealing leg: samples (0 skips it)")
     ap.add_argument("--pimc-samples", type=int, default=65536,
                     help="path-integral (SQA) annealing leg: samples (0 skips it)")
+    ap.add_argument("--dense-reads", type=int, default=1000,
+                    help="dense n=100 leg (1000 geometric sweeps): reads (0 skips it)")
+    ap.add_argument("--lattice-reads", type=int, default=256,
+                    help="3D lattice L=32 leg (4096 linear sweeps): reads (0 skips it)")
     return ap.parse_args()
 
 
@@ -90,11 +90,6 @@ def max_over_ranks(x: float, world: int, device=None) -> float:
     t = torch.tensor([float(x)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
-
-
-def full_workload(args) -> bool:
-    return (args.problems == 512 and args.sweep_scale == 1.0
-            and not getattr(args, "n_range", None) and not getattr(args, "reads_range", None))
 
 
 def workload(args, rank=0):
@@ -137,11 +132,15 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def cpu_sample(probs, budget_s, threads=None, max_reads=None):
+def cpu_sample(probs, budget_s, threads=None, max_reads=None, gpu_out=None):
     """Time the reference's own CPU implementation (the extension built from
     its sources) -- or the C restatement when that build is absent -- on a
     bounded sample of reads of the same workload, all host threads, one read
-    per call (num_samples=1, seed = that read's seed)."""
+    per call (num_samples=1, seed = that read's seed).
+
+    ``gpu_out`` = (states, energies, state_offsets, read_offsets) of the GPU
+    run of the same batch: every sampled read's reference result is then
+    compared with the GPU's, bit for bit (``checked_reads`` / ``mismatches``)."""
     import oracle
     from concurrent.futures import ThreadPoolExecutor
     threads = threads or cpu_threads()
@@ -151,6 +150,8 @@ def cpu_sample(probs, budget_s, threads=None, max_reads=None):
     order = [(int(p), 0) for p in rng.permutation(len(probs))]
     lists = {}
 
+    results = {}
+
     def one(item):
         p, r = item
         P = probs[p]
@@ -159,11 +160,12 @@ def cpu_sample(probs, budget_s, threads=None, max_reads=None):
                 lists[p] = (list(map(float, P.h)), list(map(int, P.u)), list(map(int, P.v)),
                             list(map(float, P.J)))
             h, u, v, J = lists[p]
-            ref.simulated_annealing(1, h, u, v, J, P.sweeps_per_beta, P.betas, int(P.seeds[r]),
-                                    P.states[r:r + 1].copy())
+            s, e = ref.simulated_annealing(1, h, u, v, J, P.sweeps_per_beta, P.betas,
+                                           int(P.seeds[r]), P.states[r:r + 1].copy())
         else:
-            oracle.run(P.h, P.u, P.v, P.J, P.states[r:r + 1], P.sweeps_per_beta, P.betas,
-                       P.seeds[r:r + 1])
+            s, e = oracle.run(P.h, P.u, P.v, P.J, P.states[r:r + 1], P.sweeps_per_beta, P.betas,
+                              P.seeds[r:r + 1])
+        results[(p, r)] = (np.asarray(s)[0].copy(), float(np.asarray(e)[0]))
         return P.sweeps_per_beta * len(P.betas) * P.n
 
     # Python-list conversion outside the timed region.
@@ -187,10 +189,23 @@ def cpu_sample(probs, budget_s, threads=None, max_reads=None):
             if max_reads is None and time.perf_counter() - t0 >= budget_s:
                 break
     dt = time.perf_counter() - t0
-    return {"value": attempts / dt, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{reads} reads (read 0 of randomly chosen problems of the same batch, "
-                      f"full schedules), {attempts:.3e} attempts in {dt:.1f} s",
-            "seconds": dt, "attempts": attempts}
+    out = {"value": attempts / dt, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"{reads} reads (read 0 of randomly chosen problems of the same batch, "
+                     f"full schedules), {attempts:.3e} attempts in {dt:.1f} s",
+           "seconds": dt, "attempts": attempts}
+    if gpu_out is not None:
+        states, energies, so, ro = gpu_out
+        bad = 0
+        for (p, r), (s_ref, e_ref) in results.items():
+            P = probs[p]
+            s_gpu = states[so[p] + r * P.n: so[p] + (r + 1) * P.n]
+            e_gpu = energies[ro[p] + r]
+            if not (np.array_equal(s_gpu, s_ref)
+                    and np.float64(e_gpu).view(np.uint64) == np.float64(e_ref).view(np.uint64)):
+                bad += 1
+        out["checked_reads"] = len(results)
+        out["mismatches"] = bad
+    return out
 
 
 # ------------------------------------------------------------- GPU helpers --
@@ -475,6 +490,65 @@ def bench_pimc(args, local, world, rank):
     return out
 
 
+def bench_single(args, local, world, rank, inst, label, calls, cpu_reads):
+    """One problem through simulated_annealing (the drop-in binding: host
+    buffers in and out), per-read seeds.  `value` = attempts / device time of
+    the sweep launches (CUDA events inside the call); `e2e` = attempts / wall
+    time of the whole call.  Median of `calls` calls.  Rank 0 also times the
+    reference's own extension (one read per call, all host threads) on
+    `cpu_reads` of the same reads and compares them with the GPU's."""
+    import oracle
+    from concurrent.futures import ThreadPoolExecutor
+    from b200sa import simulated_annealing
+    gibbs = inst.proposal.lower() == "gibbs"
+    kern, wall, stats = [], [], {}
+    s = e = None
+    for _ in range(calls):
+        st = inst.states.copy()
+        stats = {}
+        t0 = time.perf_counter()
+        s, e = simulated_annealing(inst.num_reads, inst.h, inst.u, inst.v, inst.J,
+                                   inst.sweeps_per_beta, inst.betas, 0, st, inst.randomize_order,
+                                   inst.proposal, seeds=inst.seeds, device=local, stats=stats)
+        wall.append(max_over_ranks(time.perf_counter() - t0, world, "cuda"))
+        kern.append(max_over_ranks(stats["kernel_ms"] / 1000.0, world, "cuda"))
+    A = inst.attempts
+    out = {"workload": label, "reads": inst.num_reads, "attempts_per_call": A,
+           "value": world * A / statistics.median(kern), "unit": UNIT,
+           "e2e": world * A / statistics.median(wall),
+           "kernel_seconds": statistics.median(kern), "call_seconds": statistics.median(wall),
+           "calls": calls, "attempts_per_pass": A / max(stats["passes"], 1),
+           "flips": stats["flips"], "near_ties": stats["near_ties"]}
+    ref = oracle.reference_module() if (rank == 0 and not args.no_cpu) else None
+    if ref is not None and cpu_reads > 0:
+        threads = cpu_threads()
+        hl, ul, vl, Jl = (list(map(float, inst.h)), list(map(int, inst.u)),
+                          list(map(int, inst.v)), list(map(float, inst.J)))
+        crit = "Gibbs" if gibbs else "Metropolis"
+
+        def one(r):  # num_samples=1, that read's seed; the binding releases the GIL
+            rs, re_ = ref.simulated_annealing(1, hl, ul, vl, Jl, inst.sweeps_per_beta, inst.betas,
+                                              int(inst.seeds[r]), inst.states[r:r + 1].copy(),
+                                              inst.randomize_order, crit)
+            return (np.array_equal(rs[0], s[r])
+                    and np.float64(re_[0]).view(np.uint64) == np.float64(e[r]).view(np.uint64))
+
+        rows = list(range(min(cpu_reads, inst.num_reads)))
+        with ThreadPoolExecutor(threads) as ex:
+            t0 = time.perf_counter()
+            same = list(ex.map(one, rows))
+            cpu = time.perf_counter() - t0
+        per_read = inst.attempts // inst.num_reads
+        out["cpu_reference"] = {"value": len(rows) * per_read / cpu, "unit": UNIT,
+                                "cores": threads, "kind": "reference",
+                                "sample": f"{len(rows)} of the same reads, one read per call"}
+        out["checked_reads"] = len(rows)
+        out["mismatches"] = int(len(rows) - sum(same))
+        out["gpu_over_cpu"] = out["value"] / out["cpu_reference"]["value"]
+        out["e2e_over_cpu"] = out["e2e"] / out["cpu_reference"]["value"]
+    return out
+
+
 def bench_bm(args, local, world):
     """Batched Boltzmann-machine learning: 64 six-regular models, n~U[256,2048],
     ground truth J*~N(0,0.5), h*=0; per gradient step 1024 fixed-beta (beta=1)
@@ -599,6 +673,11 @@ def run_ours(args):
     ms_step = total_ms / args.steps
     value = world * attempts / (ms_step / 1000.0)
 
+    # Per-bucket device times of the last timed step (events around each
+    # bucket's launch, captured into the graph) and their counters.
+    buckets = plan.bucket_report()
+    gpu_out = (sout.cpu().numpy(), en.cpu().numpy(), plan.state_offsets, plan.read_offsets)
+
     # Counters of the last warm-up run (deterministic for these inputs).
     if args.mode not in run_stats:
         run_stats[args.mode] = plan.run(sin, sout, en, mode=args.mode, stream=stream, sync=True)
@@ -618,13 +697,25 @@ def run_ours(args):
             "autotune": tune},
     }
     peak, peak_src = measured_hbm_peak()
-    abytes = algorithmic_bytes(probs, flips)
-    achieved = abytes / (ms_step / 1000.0) / 1e9
-    line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                        "frac": achieved / peak,
-                        "traffic": (TRAFFIC_BYTES_PER_STEP if full_workload(args) else None),
-                        "peak_source": peak_src,
-                        "algorithmic_bytes_per_launch": abytes}
+    timed_b = [b for b in buckets if b["ms"] > 0]
+    dom = max(timed_b, key=lambda b: b["ms"]) if timed_b else None
+    if dom is not None:
+        achieved = dom["model_bytes"] / (dom["ms"] / 1000.0) / 1e9
+        line["roofline"] = {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+            "kernel": f"sweep launch of the n<={dom['max_n']} bucket (state location "
+                      f"{dom['staging']}, {dom['registers']} registers, {dom['warps_per_cta']} "
+                      f"warps per CTA, grid {dom['grid']})",
+            "algorithmic_bytes_per_launch": dom["model_bytes"], "launch_ms": dom["ms"],
+            "note": "algorithmic bytes = the sweep's state accesses (delta energies, spins, "
+                    "adjacency), mostly served from shared memory, L1 and L2; the sweep is a "
+                    "latency-bound sequential chain per read, not HBM-bound",
+            "step_achieved_gbs": algorithmic_bytes(probs, flips) / (ms_step / 1000.0) / 1e9}
+    line["buckets"] = [{k: b[k] for k in ("max_n", "kind", "reads", "attempts", "ms", "staging",
+                                          "warps_per_cta", "registers")}
+                       | {"attempts_per_pass": b["attempts"] / max(b["passes"], 1)}
+                       for b in buckets]
     line["clocks"] = clk.summary()
     line["gpu_launches"] = args.steps * int(stats["launches"])
     line["counters"] = {"flips": flips, "near_ties": stats["near_ties"],
@@ -632,11 +723,22 @@ def run_ours(args):
                         "check_run_kernel_ms": stats["kernel_ms"]}
 
     if not args.no_plain:
-        # Same kernels as the persistent runs above (already loaded and warm).
-        plain_ms = max_over_ranks(timed("plain", 0, args.plain_steps), world, "cuda") / args.plain_steps
+        # One launch per problem, problems in order.  "plain" gives every launch
+        # the autotuned shape of its size bucket (so the ratio measures the
+        # batching alone); "plain_untuned" uses the occupancy rule.
+        plain_ms = max_over_ranks(timed("plain_tuned", 0, args.plain_steps), world,
+                                  "cuda") / args.plain_steps
         line["plain"] = {"value": world * attempts / (plain_ms / 1000.0), "ms_per_step": plain_ms,
-                         "launches_per_step": len(probs)}
+                         "launches_per_step": len(probs),
+                         "shapes": "autotuned per size bucket, as the batched run"}
         line["batched_over_plain"] = plain_ms / ms_step
+        if not args.no_tune:
+            pu_ms = max_over_ranks(timed("plain", 0, args.plain_steps), world,
+                                   "cuda") / args.plain_steps
+            line["plain_untuned"] = {"value": world * attempts / (pu_ms / 1000.0),
+                                     "ms_per_step": pu_ms, "launches_per_step": len(probs),
+                                     "shapes": "occupancy rule (no autotuning)"}
+            line["batched_over_plain_untuned"] = pu_ms / ms_step
 
     # End to end through the C ABI with host buffers (pack + H2D + anneal + D2H).
     bi, bo = h2d_d2h_bytes(probs)
@@ -658,6 +760,23 @@ def run_ours(args):
 
     plan.close()
     del sin, sout, en
+    if args.dense_reads > 0:
+        inst = workloads.dense_ising(reads=args.dense_reads)
+        lab = ("dense n=100, edge p=0.5, J,h~U[-1,1], {} reads x 1000 geometric sweeps 0.1->4.2, "
+               "Metropolis, {} order")
+        line["dense100"] = bench_single(args, local, world, rank, inst,
+                                        lab.format(args.dense_reads, "sequential"), 3,
+                                        args.dense_reads)
+        inst.randomize_order = True
+        line["dense100_random"] = bench_single(args, local, world, rank, inst,
+                                               lab.format(args.dense_reads, "random"), 3,
+                                               args.dense_reads)
+    if args.lattice_reads > 0:
+        inst = workloads.cubic_lattice(reads=args.lattice_reads)
+        line["lattice32"] = bench_single(
+            args, local, world, rank, inst,
+            f"3D periodic cubic lattice L=32 (32768 spins), J=+-1, h=0, {args.lattice_reads} reads "
+            "x 4096 linear sweeps 0.1->3.0, Metropolis, sequential order", 1, cpu_threads())
     if args.bm_steps > 0:
         line["bm"] = bench_bm(args, local, world)
     if args.descent_samples > 0:
@@ -668,8 +787,9 @@ def run_ours(args):
         line["pimc"] = bench_pimc(args, local, world, rank)
 
     if rank == 0 and not args.no_cpu:
-        cb = cpu_sample(probs, args.cpu_budget)
-        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cb = cpu_sample(probs, args.cpu_budget, gpu_out=gpu_out)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample",
+                                                   "checked_reads", "mismatches")}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

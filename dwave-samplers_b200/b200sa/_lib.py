@@ -28,6 +28,7 @@ RANDOM = 1
 MODE_PERSISTENT = 0
 MODE_PLAIN = 1
 MODE_GRAPH = 2
+MODE_PLAIN_TUNED = 3
 TUNE_FORCE = 1
 
 EXPORTS = (
@@ -44,6 +45,7 @@ EXPORTS = (
     "b200sa_random_states",
     "b200sa_plan_set_weights",
     "b200sa_plan_autotune",
+    "b200sa_plan_bucket_report",
     "b200sa_steepest_descent",
     "b200sa_rotor_anneal",
     "b200sa_path_anneal",
@@ -59,10 +61,12 @@ class Stats(ctypes.Structure):
         ("passes", ctypes.c_int64),
         ("kernel_ms", ctypes.c_double),
         ("launches", ctypes.c_int64),
+        ("read_near_ties", ctypes.c_void_p),  # input: optional per-read uint32 array
     ]
 
     def as_dict(self) -> dict:
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        return {name: getattr(self, name) for name, _ in self._fields_
+                if name != "read_near_ties"}
 
 
 class Problem(ctypes.Structure):
@@ -117,6 +121,27 @@ class TuneEntry(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BucketReport(ctypes.Structure):
+    _fields_ = [
+        ("bucket", ctypes.c_int32),
+        ("kind", ctypes.c_int32),
+        ("max_n", ctypes.c_int32),
+        ("reads", ctypes.c_int64),
+        ("attempts", ctypes.c_int64),
+        ("flips", ctypes.c_int64),
+        ("passes", ctypes.c_int64),
+        ("model_bytes", ctypes.c_double),
+        ("ms", ctypes.c_double),
+        ("staging", ctypes.c_int32),
+        ("warps_per_cta", ctypes.c_int32),
+        ("grid", ctypes.c_int32),
+        ("registers", ctypes.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 INTERRUPT_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p)
 
 _lib = None
@@ -161,7 +186,8 @@ def load() -> ctypes.CDLL:
     L.b200sa_sample_noalloc.argtypes = [
         c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32,
         c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32, c.c_int32, c.c_void_p, c.c_void_p,
-        c.c_int32, c.c_int32, c.c_int32, c.c_void_p, c.c_char_p, c.c_size_t]
+        c.c_int32, c.c_int32, c.c_int32, c.c_void_p, c.c_void_p, c.POINTER(c.c_int64),
+        c.c_char_p, c.c_size_t]
     L.b200sa_edge_moments.restype = c.c_int
     L.b200sa_edge_moments.argtypes = [c.POINTER(MomentsProblem), c.c_int32, c.c_int32,
                                       c.c_void_p, c.c_char_p, c.c_size_t]
@@ -174,6 +200,9 @@ def load() -> ctypes.CDLL:
     L.b200sa_plan_autotune.restype = c.c_int
     L.b200sa_plan_autotune.argtypes = [c.c_void_p, c.c_char_p, c.c_int32, c.POINTER(TuneEntry),
                                        c.c_int32, c.c_char_p, c.c_size_t]
+    L.b200sa_plan_bucket_report.restype = c.c_int
+    L.b200sa_plan_bucket_report.argtypes = [c.c_void_p, c.POINTER(BucketReport), c.c_int32,
+                                            c.c_char_p, c.c_size_t]
     L.b200sa_steepest_descent.restype = c.c_int
     L.b200sa_steepest_descent.argtypes = [
         c.c_int32, c.c_void_p, c.c_int64, c.c_void_p, c.c_void_p, c.c_void_p, c.c_int32,

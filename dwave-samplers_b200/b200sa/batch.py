@@ -16,7 +16,8 @@ import numpy as np
 from . import _lib
 from .workloads import Instance
 
-MODES = {"persistent": _lib.MODE_PERSISTENT, "plain": _lib.MODE_PLAIN, "graph": _lib.MODE_GRAPH}
+MODES = {"persistent": _lib.MODE_PERSISTENT, "plain": _lib.MODE_PLAIN, "graph": _lib.MODE_GRAPH,
+         "plain_tuned": _lib.MODE_PLAIN_TUNED}
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
 
 
@@ -77,16 +78,23 @@ class _Packed:
 
 def sample_batch(problems: Sequence[Instance], mode: str = "persistent", device: int = 0,
                  stats: dict | None = None) -> list[np.ndarray]:
-    """Anneal every problem's ``states`` in place; returns per-problem energies."""
+    """Anneal every problem's ``states`` in place; returns per-problem energies.
+
+    ``stats`` (a dict) receives the run's counters and ``near_ties_per_read``,
+    one array per problem with each read's near-tie count."""
     packed = _Packed(problems, need_states=True)
     L = _lib.load()
     st = _lib.Stats()
+    ties = np.zeros(sum(p.num_reads for p in problems), dtype=np.uint32)
+    st.read_near_ties = ties.ctypes.data
     err = _lib.errbuf()
     rc = L.b200sa_sample_batch(packed.arr, len(problems), MODES[mode], int(device),
                                ctypes.byref(st), err, len(err))
     _lib.check(rc, err)
     if stats is not None:
         stats.update(st.as_dict())
+        offs = np.cumsum([0] + [p.num_reads for p in problems])
+        stats["near_ties_per_read"] = [ties[offs[i]:offs[i + 1]] for i in range(len(problems))]
     return packed.energies
 
 
@@ -119,14 +127,20 @@ class Plan:
         self.attempts = int(sum(p.attempts for p in problems))
 
     def run(self, states_in, states_out, energies, seeds=None, mode: str = "persistent",
-            stream=None, sync: bool = True) -> dict:
+            stream=None, sync: bool = True, per_read: bool = False) -> dict:
         """Anneal on the device.  Arguments are CUDA tensors (or raw device
-        pointers as ints).  Returns the run's counters when ``sync``."""
+        pointers as ints).  Returns the run's counters when ``sync``; with
+        ``per_read`` also ``near_ties_per_read`` (one count per read, at the
+        plan's read offsets)."""
         def ptr(x):
             if x is None:
                 return None
             return x if isinstance(x, int) else x.data_ptr()
         st = _lib.Stats()
+        ties = None
+        if per_read and sync:
+            ties = np.zeros(self.total_reads, dtype=np.uint32)
+            st.read_near_ties = ties.ctypes.data
         err = _lib.errbuf()
         s = None
         if stream is not None:
@@ -137,7 +151,10 @@ class Plan:
                                        ptr(states_out), ptr(energies), ptr(seeds), s,
                                        1 if sync else 0, ctypes.byref(st), err, len(err))
         _lib.check(rc, err)
-        return st.as_dict()
+        out = st.as_dict()
+        if ties is not None:
+            out["near_ties_per_read"] = ties
+        return out
 
     def set_weights(self, problem: int, h, J):
         """Replace problem ``problem``'s fields and coupler weights (COO order
@@ -159,6 +176,17 @@ class Plan:
         path = cache_path.encode() if cache_path else None
         rc = self._lib.b200sa_plan_autotune(self.handle, path, _lib.TUNE_FORCE if force else 0,
                                             rep, cap, err, len(err))
+        _lib.check(rc, err)
+        return [rep[i].as_dict() for i in range(min(rc, cap))]
+
+    def bucket_report(self) -> list[dict]:
+        """Per size bucket of the last persistent or graph run: reads,
+        attempts, flips, passes, the state-access model bytes, the launch's
+        device time (ms) and its shape.  Waits for the run."""
+        cap = 64
+        rep = (_lib.BucketReport * cap)()
+        err = _lib.errbuf()
+        rc = self._lib.b200sa_plan_bucket_report(self.handle, rep, cap, err, len(err))
         _lib.check(rc, err)
         return [rep[i].as_dict() for i in range(min(rc, cap))]
 

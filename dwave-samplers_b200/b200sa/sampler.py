@@ -232,13 +232,20 @@ class SimulatedAnnealingSampler:
             beta_schedule)
 
         timestamp_sample = perf_counter_ns()
+        run = {}
         samples, energies = simulated_annealing(
             num_reads, problem.h, problem.u, problem.v, problem.J, num_sweeps_per_beta,
             beta_schedule, seed, init, randomize_order, proposal_acceptance_criteria,
-            interrupt_function, device=self.device)
+            interrupt_function, device=self.device, stats=run)
         timestamp_postprocess = perf_counter_ns()
 
         info = {"beta_range": beta_range, "beta_schedule_type": beta_schedule_type}
+        # Reads whose exp() decisions all fell outside the 2^-48 band around
+        # their thresholds are bit-exact with the reference; the others are
+        # listed (expected: none).
+        ties = run.get("near_ties_per_read", np.zeros(0, np.uint32))
+        info["near_ties"] = int(ties.sum())
+        info["near_tie_reads"] = np.flatnonzero(ties).tolist()
         if problem.vartype == "BINARY":
             out = ((np.asarray(samples) + 1) // 2).astype(np.int8)
         else:

@@ -48,7 +48,11 @@ def simulated_annealing(num_samples, h, coupler_starts, coupler_ends,
     Parameters follow ``simulated_annealing.pyx:45-130``; the keyword-only
     extras are ``seeds`` (one uint64 seed per read), ``rng_stream``
     ("per_read" or "shared"), ``device`` and ``stats`` (a dict that receives
-    the run's counters: attempts, flips, near_ties, passes, kernel_ms).
+    the run's counters: attempts, flips, near_ties, passes, kernel_ms, and
+    ``near_ties_per_read``, one count per completed read: a read with a
+    nonzero count made an exp() decision so close to its threshold that the
+    host libm could have decided it differently; every other read is
+    bit-exact with the reference).
 
     Returns views ``states_numpy[:num]`` and ``energies[:num]``, ``num`` being
     the number of reads completed (fewer when ``interrupt_function`` stops the
@@ -130,6 +134,8 @@ def simulated_annealing(num_samples, h, coupler_starts, coupler_ends,
 
     L = _lib.load()
     st = _lib.Stats()
+    read_ties = np.zeros(num_samples, dtype=np.uint32)
+    st.read_near_ties = read_ties.ctypes.data
     err = _lib.errbuf()
     rc = L.b200sa_sample(
         num_vars, hh.ctypes.data, cw.shape[0], cs.ctypes.data, ce.ctypes.data,
@@ -140,4 +146,5 @@ def simulated_annealing(num_samples, h, coupler_starts, coupler_ends,
     num = _lib.check(rc, err)
     if stats is not None:
         stats.update(st.as_dict())
+        stats["near_ties_per_read"] = read_ties[:num]
     return states_numpy[:num], energies[:num]

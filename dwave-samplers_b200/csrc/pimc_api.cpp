@@ -49,6 +49,8 @@ extern "C" int b200sa_path_anneal(
         breaks_in_size < 0 || breaks_out_size < 0)
         return set_err(err, errlen, B200SA_EINVAL, "negative size");
     if (num_samples == 0 || num_vars == 0) {  // pimc_annealing.pyx:185-191
+        if (num_samples > 0 && !energies)
+            return set_err(err, errlen, B200SA_EINVAL, "energies is NULL");
         for (int32_t r = 0; r < num_samples; ++r) energies[r] = 0.0;
         return num_samples;
     }

@@ -71,6 +71,15 @@ struct DevArray {
 
 inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
+// Zeroes the counters of a b200sa_stats, keeping the caller's per-read
+// near-tie array pointer (an input).
+inline void reset_stats(b200sa_stats *s) {
+    if (!s) return;
+    uint32_t *keep = s->read_near_ties;
+    *s = b200sa_stats{};
+    s->read_near_ties = keep;
+}
+
 // Nibble tables of the RNG jump by kHalf outputs (computed once per process).
 const uint32_t (*jump_table())[4];
 
@@ -165,9 +174,18 @@ struct b200sa_plan_s {
     cudaGraphExec_t graph_exec = nullptr;
     const void *graph_key[4] = {};
     int64_t graph_launches = 0;
+    // Timing events around each bucket's launch (recorded on the bucket's
+    // stream by persistent runs, and captured into the graph), and the shape
+    // of that launch; bucket_timed marks buckets the last such run launched.
+    cudaEvent_t bev[b200sa::host::kBuckets][2] = {};
+    b200sa::host::LaunchShape bshape[b200sa::host::kBuckets] = {};
+    bool bucket_timed[b200sa::host::kBuckets] = {};
 
     ~b200sa_plan_s() {
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        for (int b = 0; b < b200sa::host::kBuckets; ++b)
+            for (int k = 0; k < 2; ++k)
+                if (bev[b][k]) cudaEventDestroy(bev[b][k]);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (fork) cudaEventDestroy(fork);

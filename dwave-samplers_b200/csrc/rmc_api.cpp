@@ -37,6 +37,8 @@ extern "C" int b200sa_rotor_anneal(int32_t num_vars, const double *h, int64_t nu
                        "proposal must be 0 (GibbsNonErgodic), 1 (MetropolisNonErgodic), "
                        "2 (MetropolisUniform) or 3 (MetropolisTF)");
     if (num_samples == 0 || num_vars == 0) {  // rotormc_annealing.pyx:161-164
+        if (num_samples > 0 && !energies)
+            return set_err(err, errlen, B200SA_EINVAL, "energies is NULL");
         for (int32_t r = 0; r < num_samples; ++r) energies[r] = 0.0;
         return num_samples;
     }

@@ -87,11 +87,12 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
         stage = kStageGlobal;
     const int cap = stage == kStageGlobal ? 0 : max_n_here;
     const int region = region_bytes_for_stage(stage, cap);
-    const int reg_class = choice && choice->set && persistent ? choice->reg_class : 0;
+    const int reg_class = choice && choice->set ? choice->reg_class : 0;
     const int variant = kernel_variant(kind & 1, kind & 2, stage, reg_class);
     out.stage = stage;
-    if (choice && choice->set && persistent) {
-        // The autotuner's measured configuration.
+    if (choice && choice->set) {
+        // The autotuner's measured configuration (a persistent launch takes
+        // items from its queue; a plain one strides over them statically).
         const int w = choice->warps_per_cta;
         if (w < 1 || w > kMaxThreadsPerCta / 32 || (int64_t)w * region > smem_blk)
             return set_err(err, errlen, B200SA_EINVAL, "tuned shape does not fit");
@@ -244,7 +245,9 @@ int collect_stats(b200sa_plan_s *P, const std::vector<std::pair<int, int>> &rang
         const int p = pr.first;
         const int64_t att_per_read = (int64_t)P->n[p] * P->sweeps[p];
         for (int r = 0; r < pr.second; ++r) {
-            const ReadStats &x = hs[(size_t)(P->read_off[p] + r)];
+            const size_t rd = (size_t)(P->read_off[p] + r);
+            const ReadStats &x = hs[rd];
+            if (stats->read_near_ties) stats->read_near_ties[rd] = x.near_ties;
             stats->flips += (int64_t)x.flips;
             stats->passes += (int64_t)x.passes;
             stats->near_ties += (int64_t)x.near_ties;
@@ -295,14 +298,18 @@ int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
     for (int i = 0; i < kBuckets; ++i) {
         const int b = order[i];
         const int64_t cnt = P->bucket_off[b + 1] - P->bucket_off[b];
+        P->bucket_timed[b] = cnt > 0;
         if (cnt <= 0) continue;
         const int si = next++ % kStreams;
         if (!used[si]) B200SA_CUDA(cudaStreamWaitEvent(P->bstream[si], P->fork, 0));
         used[si] = true;
+        B200SA_CUDA(cudaEventRecord(P->bev[b][0], P->bstream[si]));
         int rc = launch_shape(P, a, shape[b], P->items_lpt.ptr + P->bucket_off[b], cnt,
                               P->bucket_max_n[b], true, false, P->qhead.ptr + b, slot0[b],
                               P->bstream[si], err, errlen);
         if (rc) return rc;
+        B200SA_CUDA(cudaEventRecord(P->bev[b][1], P->bstream[si]));
+        P->bshape[b] = shape[b];
     }
     for (int si = 0; si < kStreams; ++si) {
         if (!used[si]) continue;
@@ -363,6 +370,8 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
     B200SA_CUDA(cudaEventCreate(&P->ev0));
     B200SA_CUDA(cudaEventCreate(&P->ev1));
     B200SA_CUDA(cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming));
+    for (int b = 0; b < kBuckets; ++b)
+        for (int k = 0; k < 2; ++k) B200SA_CUDA(cudaEventCreate(&P->bev[b][k]));
     P->num_problems = num_problems;
     // On chip when at least three warps' regions fit in one SM.
     {
@@ -566,14 +575,15 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
                     void *stream, int32_t sync, b200sa_stats *stats, char *err,
                     size_t errlen) {
     if (!plan) return set_err(err, errlen, B200SA_EINVAL, "plan is NULL");
-    if (mode != B200SA_MODE_PERSISTENT && mode != B200SA_MODE_PLAIN && mode != B200SA_MODE_GRAPH)
+    if (mode != B200SA_MODE_PERSISTENT && mode != B200SA_MODE_PLAIN && mode != B200SA_MODE_GRAPH &&
+        mode != B200SA_MODE_PLAIN_TUNED)
         return set_err(err, errlen, B200SA_EINVAL, "unknown mode");
     if (plan->total_reads > 0 && (!d_states_in || !d_states_out || !d_energies))
         return set_err(err, errlen, B200SA_EINVAL, "device buffers are NULL");
     DeviceGuard guard;
     B200SA_CUDA(cudaSetDevice(plan->device));
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
-    if (stats) std::memset(stats, 0, sizeof(*stats));
+    reset_stats(stats);
     LaunchArgs a = base_args(plan, d_states_in, d_states_out, d_energies, d_seeds);
     plan->launches = 0;
     // Problems with no variables: energies are 0 (cpu_sa.cpp:217-226 over nothing).
@@ -589,11 +599,18 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
     } else if (mode == B200SA_MODE_GRAPH) {
         rc = run_graph(plan, a, st, err, errlen);
     } else {
+        // One launch per problem; PLAIN_TUNED gives each launch the tuned
+        // shape of the problem's bucket (its size class and kind).
+        const bool tuned = mode == B200SA_MODE_PLAIN_TUNED;
         for (int i = 0; i < plan->num_problems && rc == B200SA_OK; ++i) {
             const int64_t o = plan->plain_item_off[i];
-            rc = launch_items(plan, a, kind_of(plan->hprobs[i]), plan->items_plain.ptr + o,
+            const int kind = kind_of(plan->hprobs[i]);
+            const TuneChoice *choice =
+                tuned ? &plan->tune[size_class(plan->n[i], plan->onchip_max) * kKinds + kind]
+                      : nullptr;
+            rc = launch_items(plan, a, kind, plan->items_plain.ptr + o,
                               plan->plain_item_off[i + 1] - o, plan->n[i], false, false,
-                              nullptr, st, err, errlen);
+                              nullptr, st, err, errlen, choice);
         }
     }
     if (rc) return rc;
@@ -608,8 +625,13 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
                 ranges.emplace_back(i, plan->n[i] ? plan->reads[i] : 0);
             rc = collect_stats(plan, ranges, stats, err, errlen);
             if (rc) return rc;
-            for (int i = 0; i < plan->num_problems; ++i)
-                if (plan->n[i] == 0) stats->reads += plan->reads[i];
+            for (int i = 0; i < plan->num_problems; ++i) {
+                if (plan->n[i] != 0) continue;
+                stats->reads += plan->reads[i];
+                if (stats->read_near_ties)
+                    for (int r = 0; r < plan->reads[i]; ++r)
+                        stats->read_near_ties[plan->read_off[i] + r] = 0;
+            }
             stats->kernel_ms = ms;
             stats->launches = plan->launches;
         }
@@ -674,7 +696,7 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
                   int32_t varorder, int32_t proposal, b200sa_interrupt_fn interrupt_fn,
                   void *interrupt_ctx, int32_t device, b200sa_stats *stats, char *err,
                   size_t errlen) {
-    if (stats) std::memset(stats, 0, sizeof(*stats));
+    reset_stats(stats);
     if (num_reads < 0) return set_err(err, errlen, B200SA_EINVAL, "num_reads < 0");
     if (num_reads == 0) return 0;
     if (!states && num_vars > 0)
@@ -712,6 +734,7 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
         if (rc) return set_err(err, errlen, rc, msg);
         for (int32_t r = 0; r < num_reads; ++r) {
             energies[r] = 0.0;
+            if (stats && stats->read_near_ties) stats->read_near_ties[r] = 0;
             if (interrupt_fn && interrupt_fn(interrupt_ctx)) {
                 if (stats) stats->reads = r + 1;
                 return r + 1;
@@ -797,6 +820,63 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
         stats->kernel_ms = total_ms;
     }
     return done;
+}
+
+int b200sa_plan_bucket_report(b200sa_plan plan, b200sa_bucket_report *out, int32_t cap,
+                              char *err, size_t errlen) {
+    if (!plan) return set_err(err, errlen, B200SA_EINVAL, "plan is NULL");
+    if (cap < 0 || (cap > 0 && !out)) return set_err(err, errlen, B200SA_EINVAL, "bad report buffer");
+    DeviceGuard guard;
+    B200SA_CUDA(cudaSetDevice(plan->device));
+    B200SA_CUDA(cudaEventSynchronize(plan->ev1));
+    std::vector<ReadStats> hs((size_t)plan->total_reads);
+    if (plan->total_reads)
+        B200SA_CUDA(cudaMemcpy(hs.data(), plan->dstats.ptr,
+                               sizeof(ReadStats) * (size_t)plan->total_reads,
+                               cudaMemcpyDeviceToHost));
+    int k = 0;
+    for (int b = 0; b < kBuckets; ++b) {
+        const int64_t o0 = plan->bucket_off[b], o1 = plan->bucket_off[b + 1];
+        if (o1 <= o0) continue;
+        if (k < cap) {
+            b200sa_bucket_report &r = out[k];
+            r = b200sa_bucket_report{};
+            r.bucket = b;
+            r.kind = b % kKinds;
+            r.max_n = plan->bucket_max_n[b];
+            for (int64_t i = o0; i < o1; ++i) {
+                const int64_t it = plan->h_items_lpt[(size_t)i];
+                const int p = (int)(it >> 32), rd = (int)(it & 0xffffffffll);
+                const ReadStats &x = hs[(size_t)(plan->read_off[p] + rd)];
+                const double n = plan->n[p], m = (double)plan->hprobs[p].m;
+                const double d = n > 0 ? 2.0 * m / n : 0.0;
+                const double att = n * (double)plan->sweeps[p];
+                r.reads += 1;
+                r.attempts += (int64_t)att;
+                r.flips += (int64_t)x.flips;
+                r.passes += (int64_t)x.passes;
+                // Per read: initial delta energies n(8 + 13d), 9 bytes per
+                // attempt, 29d + 9 per flip, final energy 9n + 14m.
+                r.model_bytes += n * (8.0 + 13.0 * d) + 9.0 * att +
+                                 (double)x.flips * (29.0 * d + 9.0) + 9.0 * n + 14.0 * m;
+            }
+            r.ms = -1.0;
+            if (plan->bucket_timed[b]) {
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, plan->bev[b][0], plan->bev[b][1]) == cudaSuccess)
+                    r.ms = ms;
+                else
+                    cudaGetLastError();
+                const LaunchShape &s = plan->bshape[b];
+                r.staging = s.stage;
+                r.warps_per_cta = s.warps_per_cta;
+                r.grid = s.grid;
+                r.registers = (s.variant >> 4) == 1 ? kRegs80 : (s.variant >> 4) == 2 ? kRegs64 : 128;
+            }
+        }
+        ++k;
+    }
+    return k;
 }
 
 }  // extern "C"

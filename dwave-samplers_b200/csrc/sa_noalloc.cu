@@ -18,8 +18,11 @@
 // and must be serialized by the caller.
 //
 // The first call on each device resolves the array's device address with
-// cudaGetSymbolAddress and uploads the RNG jump table; make that first call
-// before any stream capture on that device.
+// cudaGetSymbolAddress, uploads the RNG jump table and reads the device's
+// properties once.  Every call waits for its own work (it reads an error flag
+// and the near-tie total back to the host), so a call cannot be recorded
+// into a CUDA graph: a call made while its stream is capturing returns
+// B200SA_EINVAL before doing anything.
 //
 // The annealing itself is the regular sweep kernel, unchanged; only its
 // inputs (packed adjacency, thresholds, work items, counters) are prepared
@@ -49,6 +52,7 @@ constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Byte offsets of the working areas inside the fixed array.
 constexpr size_t kOffErr = 0;                                      // int error flag
+constexpr size_t kOffTies = 64;                                    // near-tie total (u64)
 constexpr size_t kOffQueue = 256;                                  // work-queue head
 constexpr size_t kOffProb = 512;                                   // ProblemDev
 constexpr size_t kOffCursor = align256(kOffProb + sizeof(ProblemDev));  // int[n]
@@ -191,11 +195,35 @@ __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
     }
 }
 
-// Per-device set-up: the array's device address and the RNG jump table.
+// Copies each read's near-tie count out of the fixed array (when the caller
+// gave a device array for them) and sums them into the total at kOffTies.
+__global__ void __launch_bounds__(1024) noalloc_ties_kernel(unsigned char *base, int num_reads,
+                                                            uint32_t *out) {
+    const ReadStats *stats = reinterpret_cast<const ReadStats *>(base + kOffStats);
+    unsigned long long *total = reinterpret_cast<unsigned long long *>(base + kOffTies);
+    __shared__ unsigned long long s_sum;
+    if (threadIdx.x == 0) s_sum = 0ull;
+    __syncthreads();
+    unsigned long long mine = 0ull;
+    for (int r = threadIdx.x; r < num_reads; r += blockDim.x) {
+        const unsigned t = stats[r].near_ties;
+        if (out) out[r] = t;
+        mine += t;
+    }
+    atomicAdd(&s_sum, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) *total = s_sum;
+}
+
+// Per-device set-up: the array's device address, the RNG jump table and the
+// device properties the launch shape needs.
 struct DeviceSetup {
     std::once_flag once;
     cudaError_t status = cudaSuccess;
     unsigned char *base = nullptr;
+    int major = 0;
+    int sms = 0;
+    size_t smem_optin = 0;
 };
 constexpr int kMaxDevices = 64;
 DeviceSetup g_setup[kMaxDevices];
@@ -219,7 +247,8 @@ extern "C" int b200sa_sample_noalloc(
     const int8_t *d_states_in, int8_t *d_states_out, double *d_energies,
     int32_t sweeps_per_beta, int32_t num_betas, const double *d_beta_schedule,
     const uint64_t *d_seeds, int32_t varorder, int32_t proposal, int32_t device,
-    void *stream, char *err, size_t errlen) {
+    void *stream, uint32_t *d_read_near_ties, int64_t *near_ties, char *err, size_t errlen) {
+    if (near_ties) *near_ties = 0;
     // Size limits of the fixed working memory, checked before any device work.
     if (num_vars < 0 || num_couplers < 0 || num_reads < 0 || num_betas < 0 ||
         sweeps_per_beta < 0)
@@ -239,11 +268,24 @@ extern "C" int b200sa_sample_noalloc(
         return fail(err, errlen, B200SA_EINVAL, "varorder must be 0 or 1");
     if (proposal != B200SA_GIBBS && proposal != B200SA_METROPOLIS)
         return fail(err, errlen, B200SA_EINVAL, "proposal must be 0 or 1");
+    {
+        // Every call ends by waiting for its work, which a stream capture
+        // does not allow: refuse before enqueuing anything.
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        const cudaError_t ce = cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap);
+        if (ce != cudaSuccess) return fail(err, errlen, B200SA_ECUDA, cudaGetErrorString(ce));
+        if (cap != cudaStreamCaptureStatusNone)
+            return fail(err, errlen, B200SA_EINVAL,
+                        "b200sa_sample_noalloc cannot be captured into a CUDA graph: it waits "
+                        "for its own work; call it outside stream capture");
+    }
     if (num_reads == 0 || num_vars == 0) {
         if (num_reads && !d_energies) return fail(err, errlen, B200SA_EINVAL, "energies is NULL");
         if (num_reads) {
             cudaStream_t st = static_cast<cudaStream_t>(stream);
             cudaError_t e = cudaMemsetAsync(d_energies, 0, sizeof(double) * (size_t)num_reads, st);
+            if (e == cudaSuccess && d_read_near_ties)
+                e = cudaMemsetAsync(d_read_near_ties, 0, sizeof(uint32_t) * (size_t)num_reads, st);
             if (e == cudaSuccess) e = cudaStreamSynchronize(st);
             if (e != cudaSuccess) return fail(err, errlen, B200SA_ECUDA, cudaGetErrorString(e));
         }
@@ -266,27 +308,32 @@ extern "C" int b200sa_sample_noalloc(
     } restore{prev};
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail(err, errlen, B200SA_ENODEV, cudaGetErrorString(e));
-    cudaDeviceProp prop;
-    e = cudaGetDeviceProperties(&prop, device);
-    if (e != cudaSuccess) return fail(err, errlen, B200SA_ECUDA, cudaGetErrorString(e));
-    if (prop.major != 10)
-        return fail(err, errlen, B200SA_ENODEV, "this library is built for sm_100a (B200)");
 
-    // Once per device, with that device current: resolve the array's device
-    // address (the host-side name is only a stand-in) and load the jump table.
+    // Once per device, with that device current: read its properties,
+    // resolve the array's device address (the host-side name is only a
+    // stand-in) and load the jump table.
     std::call_once(g_jump_once, [] {
         uint32_t cols[128][4];
         rng_jump_columns(kHalf, cols);
         rng_jump_nibbles(cols, g_jump_table);
     });
     DeviceSetup &S = g_setup[device];
-    std::call_once(S.once, [&S] {
+    std::call_once(S.once, [&S, device] {
+        cudaDeviceProp prop;
+        S.status = cudaGetDeviceProperties(&prop, device);
+        if (S.status != cudaSuccess) return;
+        S.major = prop.major;
+        S.sms = prop.multiProcessorCount;
+        S.smem_optin = prop.sharedMemPerBlockOptin;
+        if (S.major != 10) return;
         void *ptr = nullptr;
         S.status = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (S.status == cudaSuccess) S.base = static_cast<unsigned char *>(ptr);
         if (S.status == cudaSuccess) S.status = upload_jump_table(g_jump_table, nullptr);
         if (S.status == cudaSuccess) S.status = cudaStreamSynchronize(nullptr);
     });
+    if (S.status == cudaSuccess && S.major != 10)
+        return fail(err, errlen, B200SA_ENODEV, "this library is built for sm_100a (B200)");
     if (S.status != cudaSuccess || !S.base)
         return fail(err, errlen, B200SA_ECUDA,
                     std::string("set-up of the fixed working memory failed: ") +
@@ -322,7 +369,7 @@ extern "C" int b200sa_sample_noalloc(
     const int region = region_bytes_for(num_vars);
     int best_w = 1, best = 0;
     for (int wpc = 1; wpc <= kMaxThreadsPerCta / 32; ++wpc) {
-        if ((size_t)wpc * (size_t)region > prop.sharedMemPerBlockOptin) break;
+        if ((size_t)wpc * (size_t)region > S.smem_optin) break;
         int ctas = 0;
         e = kernel_occupancy(variant, wpc, region, &ctas);
         if (e != cudaSuccess) return fail(err, errlen, B200SA_ECUDA, cudaGetErrorString(e));
@@ -332,13 +379,12 @@ extern "C" int b200sa_sample_noalloc(
         }
     }
     if (best == 0) return fail(err, errlen, B200SA_ECUDA, "kernel does not fit on an SM");
-    const int wpc = (int)std::min<int64_t>(best_w, (num_reads + prop.multiProcessorCount - 1) /
-                                                       prop.multiProcessorCount);
+    const int wpc = (int)std::min<int64_t>(best_w, (num_reads + S.sms - 1) / S.sms);
     int ctas = 0;
     e = kernel_occupancy(variant, wpc, region, &ctas);
     if (e != cudaSuccess) return fail(err, errlen, B200SA_ECUDA, cudaGetErrorString(e));
     const int grid = (int)std::max<int64_t>(
-        1, std::min<int64_t>((int64_t)prop.multiProcessorCount * ctas, (num_reads + wpc - 1) / wpc));
+        1, std::min<int64_t>((int64_t)S.sms * ctas, (num_reads + wpc - 1) / wpc));
 
     LaunchArgs a{};
     a.problems = reinterpret_cast<const ProblemDev *>(S.base + kOffProb);
@@ -352,7 +398,15 @@ extern "C" int b200sa_sample_noalloc(
     a.stats = reinterpret_cast<ReadStats *>(S.base + kOffStats);
     a.smem_cap_n = num_vars;
     e = launch_sa(variant, a, grid, wpc, region, st);
+    if (e == cudaSuccess) {
+        noalloc_ties_kernel<<<1, 1024, 0, st>>>(S.base, num_reads, d_read_near_ties);
+        e = cudaGetLastError();
+    }
+    unsigned long long ties = 0ull;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&ties, S.base + kOffTies, sizeof(ties), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail(err, errlen, B200SA_ECUDA, cudaGetErrorString(e));
+    if (near_ties) *near_ties = (int64_t)ties;
     return num_reads;
 }

@@ -60,6 +60,8 @@ extern "C" {
 #define B200SA_MODE_PLAIN 1      /* one launch per problem, problems in order */
 #define B200SA_MODE_GRAPH 2      /* the persistent launches captured once as a CUDA graph
                                     (plans only; replayed while the buffers are the same) */
+#define B200SA_MODE_PLAIN_TUNED 3 /* one launch per problem, each with the autotuned shape
+                                     of its size bucket (plain batching with tuned launches) */
 
 /* Replaces the reference's `callback` (cpu_sa.h:61): called between reads,
  * in read order, for each completed read; nonzero stops sampling and the
@@ -74,6 +76,16 @@ typedef struct {
     int64_t passes;       /* warp passes of the sequential sweep (speculation efficiency) */
     double kernel_ms;     /* device time of the sampling launches (CUDA events) */
     int64_t launches;     /* sweep-kernel launches issued */
+    /* Input, optional (NULL: not wanted): a caller-owned host array that
+     * receives each completed read's near-tie count, one uint32 per read, in
+     * read order (b200sa_sample: num_reads entries; b200sa_sample_batch and
+     * b200sa_plan_run: every read of every problem, at the plan's read
+     * offsets).  A read with a nonzero count made an exp() decision within
+     * 2^-48 of its threshold, where CUDA's exp and the host libm's could
+     * decide differently; every other read is bit-exact with the reference.
+     * Entries of reads that did not complete are left untouched.  The call
+     * keeps this pointer when it resets the counters above. */
+    uint32_t *read_near_ties;
 } b200sa_stats;
 
 /* One binary quadratic model in Ising form plus its reads.
@@ -194,6 +206,34 @@ typedef struct {
 B200SA_API int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags,
                                     b200sa_tune_entry *report, int32_t report_cap, char *err,
                                     size_t errlen);
+
+/* Per-bucket figures of a plan's last persistent or graph run (no reference
+ * counterpart).  Buckets group the reads by size class and kernel kind; each
+ * is one launch.  ms is that launch's device time (CUDA events on the
+ * bucket's stream, captured into the graph in graph mode; -1 when unknown),
+ * model_bytes the bytes the sweep's state accesses amount to (per read: the
+ * initial delta energies n(8 + 13d), 9 per attempt, 29d + 9 per flip and
+ * the final energy 9n + 14m, d the mean list length), most of them served
+ * from shared memory, L1 and L2.  Waits for the run.  Returns the number of
+ * non-empty buckets (up to cap entries written) or a negative error. */
+typedef struct {
+    int32_t bucket;
+    int32_t kind;           /* bit 0 Gibbs, bit 1 random order */
+    int32_t max_n;
+    int64_t reads;
+    int64_t attempts;
+    int64_t flips;
+    int64_t passes;
+    double model_bytes;
+    double ms;
+    int32_t staging;        /* state location of the launch (see b200sa_tune_entry) */
+    int32_t warps_per_cta;
+    int32_t grid;
+    int32_t registers;
+} b200sa_bucket_report;
+
+B200SA_API int b200sa_plan_bucket_report(b200sa_plan plan, b200sa_bucket_report *out,
+                                         int32_t cap, char *err, size_t errlen);
 
 /* ---- Steepest descent ---------------------------------------------------------
  * Replaces steepest_gradient_descent (dwave/samplers/greedy/src/descent.cpp:
@@ -333,16 +373,22 @@ B200SA_API int b200sa_random_states(uint64_t init_seed, uint64_t model_index, in
  * only (read r equals a reference call with num_samples=1, seed=seeds[r]).
  * All calls on a device share that array: calls that overlap on the GPU race
  * and must be serialized by the caller.  The first call on a device sets the
- * array up (device address, RNG tables); make it before any stream capture.
- * `stream` is a cudaStream_t (NULL = legacy default stream); the call returns
- * when the work is complete.  Returns num_reads or a negative error. */
+ * array up (device address, RNG tables, device properties).  `stream` is a
+ * cudaStream_t (NULL = legacy default stream); the call returns when the work
+ * is complete, so it cannot be recorded into a CUDA graph (a call on a
+ * capturing stream returns B200SA_EINVAL).  Near ties: d_read_near_ties
+ * (optional DEVICE array, num_reads entries) receives each read's count of
+ * exp() decisions within 2^-48 of their threshold, and near_ties (optional
+ * host pointer) their total; a read with a nonzero count may differ from the
+ * reference, every other read is bit-exact.  Returns num_reads or a negative
+ * error. */
 B200SA_API int b200sa_sample_noalloc(
     int32_t num_vars, const double *d_h, int64_t num_couplers, const int32_t *d_coupler_starts,
     const int32_t *d_coupler_ends, const double *d_coupler_weights, int32_t num_reads,
     const int8_t *d_states_in, int8_t *d_states_out, double *d_energies,
     int32_t sweeps_per_beta, int32_t num_betas, const double *d_beta_schedule,
     const uint64_t *d_seeds, int32_t varorder, int32_t proposal, int32_t device, void *stream,
-    char *err, size_t errlen);
+    uint32_t *d_read_near_ties, int64_t *near_ties, char *err, size_t errlen);
 
 /* Diagnostic, no reference counterpart: checks on the device that the
  * single-precision acceptance bounds used before the exact double-precision

@@ -190,7 +190,25 @@ def test_every_configuration_gives_identical_results(tmp_path):
             with Plan(probs) as plan:
                 rep = plan.autotune(str(cache))
                 assert all(e["from_cache"] == 1 for e in rep)
-                out = torch.empty_like(ref)
-                en = torch.empty_like(en_ref)
-                plan.run(sin, out, en)
-                assert torch.equal(out, ref) and torch.equal(en, en_ref), (staging, regs)
+                for mode in ("persistent", "plain_tuned"):
+                    out = torch.empty_like(ref)
+                    en = torch.empty_like(en_ref)
+                    plan.run(sin, out, en, mode=mode)
+                    assert torch.equal(out, ref) and torch.equal(en, en_ref), (staging, regs, mode)
+
+
+def test_bucket_report_matches_run_counters():
+    """Per-bucket figures of a persistent run and of a graph replay add up to
+    the run's counters, and each bucket launch has a device time."""
+    probs = workloads.uneven_batch(num_problems=10, n_range=(64, 3000), reads_range=(8, 40),
+                                   sweeps_range=(10, 30), seed=61)
+    with Plan(probs) as plan:
+        sin, out, en = device_buffers(plan, probs)
+        for mode in ("persistent", "graph"):
+            st = plan.run(sin, out, en, mode=mode)
+            rep = plan.bucket_report()
+            assert rep and sum(r["reads"] for r in rep) == plan.total_reads
+            assert sum(r["attempts"] for r in rep) == st["attempts"]
+            assert sum(r["flips"] for r in rep) == st["flips"]
+            assert sum(r["passes"] for r in rep) == st["passes"]
+            assert all(r["ms"] > 0 and r["model_bytes"] > 0 and r["grid"] > 0 for r in rep), rep

@@ -18,6 +18,8 @@ def test_ground_state_ferromagnet_and_timing():
     for k in ("preprocessing_ns", "sampling_ns", "postprocessing_ns"):
         assert ss.info["timing"][k] > 0
     assert "beta_range" in ss.info and ss.info["beta_schedule_type"] == "geometric"
+    # No read decided an exp() comparison inside the cross-libm tie band.
+    assert ss.info["near_ties"] == 0 and ss.info["near_tie_reads"] == []
     assert Neal is SimulatedAnnealingSampler
 
 
