@@ -6,6 +6,8 @@ Public surface:
   (``dwave/samplers/sa/simulated_annealing.pyx``).
 * :func:`sample_batch`, :class:`Plan` -- many problems in one persistent
   launch (graph replay, in-place weights, autotuning).
+* :mod:`b200sa.shards` -- one batch split across several GPUs (threads of
+  one process, or one rank per GPU under torch.distributed).
 * :mod:`b200sa.sampler` -- ``SimulatedAnnealingSampler`` front end (dimod-free).
 * :mod:`b200sa.greedy` -- steepest descent (``dwave.samplers.greedy``).
 * :mod:`b200sa.sqa` -- ``dwave.samplers.sqa``'s two bindings: rotor-model

@@ -44,6 +44,7 @@ EXPORTS = (
     "b200sa_edge_moments",
     "b200sa_random_states",
     "b200sa_plan_set_weights",
+    "b200sa_plan_set_weights_device",
     "b200sa_plan_autotune",
     "b200sa_plan_bucket_report",
     "b200sa_steepest_descent",
@@ -197,6 +198,9 @@ def load() -> ctypes.CDLL:
     L.b200sa_plan_set_weights.restype = c.c_int
     L.b200sa_plan_set_weights.argtypes = [c.c_void_p, c.c_int32, c.c_void_p, c.c_void_p,
                                           c.c_char_p, c.c_size_t]
+    L.b200sa_plan_set_weights_device.restype = c.c_int
+    L.b200sa_plan_set_weights_device.argtypes = [c.c_void_p, c.c_void_p, c.c_void_p, c.c_void_p,
+                                                 c.c_char_p, c.c_size_t]
     L.b200sa_plan_autotune.restype = c.c_int
     L.b200sa_plan_autotune.argtypes = [c.c_void_p, c.c_char_p, c.c_int32, c.POINTER(TuneEntry),
                                        c.c_int32, c.c_char_p, c.c_size_t]

@@ -120,11 +120,30 @@ class ModelSampler:
 
     def sample(self, hs, Js, seed: int, init_seed: int, read0: int = 0) -> list[torch.Tensor]:
         """One int8 CUDA tensor (reads x n) per model; the tensors are views of
-        the sampler's output buffer, overwritten by the next call."""
+        the sampler's output buffer, overwritten by the next call.  ``hs`` /
+        ``Js`` are per-model arrays (host or device)."""
+        dev = self.sin.device
+        cat = lambda xs: torch.cat([torch.as_tensor(x, dtype=torch.float64).reshape(-1).to(dev)
+                                    for x in xs]) if len(xs) else torch.zeros(0, dtype=torch.float64,
+                                                                              device=dev)
+        return self.sample_cat(cat(hs), cat(Js), seed, init_seed, read0)
+
+    def sample_cat(self, h_cat: torch.Tensor, J_cat: torch.Tensor, seed: int, init_seed: int,
+                   read0: int = 0) -> list[torch.Tensor]:
+        """As :meth:`sample`, with every model's fields and couplings given
+        concatenated in two float64 CUDA tensors: they are written into the
+        plan on the device (``b200sa_plan_set_weights_device``), with no host
+        round trip."""
         dev = self.sin.device
         offs = self.plan.state_offsets
-        for k, (h, J) in enumerate(zip(hs, Js)):
-            self.plan.set_weights(k, h, J)
+        stream = torch.cuda.current_stream(dev)
+        h_cat = h_cat.detach().to(device=dev, dtype=torch.float64).contiguous()
+        J_cat = J_cat.detach().to(device=dev, dtype=torch.float64).contiguous()
+        if h_cat.numel() == 0:
+            h_cat = torch.zeros(1, dtype=torch.float64, device=dev)
+        if J_cat.numel() == 0:
+            J_cat = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.plan.set_weights_device(h_cat, J_cat, stream=stream)
         seeds = np.concatenate([read_seeds(seed, k, self.reads, read0)
                                 for k in range(len(self.models))])
         self.seeds[:seeds.shape[0]].copy_(torch.from_numpy(seeds.view(np.int64)))
@@ -208,16 +227,18 @@ class LogPartition(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, h_cat, J_cat, spec):
-        hs, Js = spec.split(h_cat.detach().cpu().numpy(), J_cat.detach().cpu().numpy())
+        # The weights stay on the device: they are scattered into the plan by
+        # a kernel (no copy to the host).
+        dev = torch.device("cuda", spec.device)
+        hd = h_cat.detach().to(device=dev, dtype=torch.float64).contiguous()
+        Jd = J_cat.detach().to(device=dev, dtype=torch.float64).contiguous()
         keep = spec.reads * sum(m.num_vars for m in spec.models) <= spec.memory_budget
         samples = []
         if keep:
-            samples = sample_models(spec.models, hs, Js, spec.beta, spec.sweeps, spec.reads,
-                                    spec.seed, spec.init_seed, 0, spec.proposal, spec.device,
-                                    spec.sampler(spec.reads))
+            samples = spec.sampler(spec.reads).sample_cat(hd, Jd, spec.seed, spec.init_seed, 0)
         spec.last_samples = samples
         ctx.spec = spec
-        ctx.hs, ctx.Js = hs, Js
+        ctx.hs, ctx.Js = hd, Jd
         ctx.samples = samples
         ctx.h_device, ctx.J_device = h_cat.device, J_cat.device
         return torch.zeros((), dtype=torch.float64, device=h_cat.device)
@@ -269,16 +290,16 @@ class SamplingSpec:
             j += m.num_couplers
         return hs, Js
 
-    def moments(self, hs, Js, samples):
+    def moments(self, h_cat, J_cat, samples):
+        """Moment sums of the forward's samples, or of samples recomputed from
+        the stored seeds (h_cat / J_cat: the concatenated weights, device)."""
         if samples:
             return edge_moments(self.models, samples, self.device)
         # Recompute from the stored seeds, chunk by chunk of reads.
         tot_s = tot_ss = None
         for r0 in range(0, self.reads, self.recompute_chunk):
             k = min(self.recompute_chunk, self.reads - r0)
-            chunk = sample_models(self.models, hs, Js, self.beta, self.sweeps, k, self.seed,
-                                  self.init_seed, r0, self.proposal, self.device,
-                                  self.sampler(k))
+            chunk = self.sampler(k).sample_cat(h_cat, J_cat, self.seed, self.init_seed, r0)
             s, ss = edge_moments(self.models, chunk, self.device)
             if tot_s is None:
                 tot_s, tot_ss = s, ss

@@ -166,6 +166,23 @@ class Plan:
                                                J.ctypes.data, err, len(err))
         _lib.check(rc, err)
 
+    def set_weights_device(self, h_cat, J_cat, stream=None):
+        """Replace the fields and coupler weights of every problem from device
+        tensors (float64 CUDA tensors: all problems' h concatenated, and all
+        problems' J in COO order concatenated), enqueued on ``stream``."""
+        for x in (h_cat, J_cat):
+            if x.dtype.itemsize != 8 or not x.is_cuda or not x.is_contiguous():
+                raise ValueError("h_cat and J_cat must be contiguous float64 CUDA tensors")
+        s = None
+        if stream is not None:
+            s = stream if isinstance(stream, int) else stream.cuda_stream
+            if s == 0:
+                s = CUDA_STREAM_LEGACY
+        err = _lib.errbuf()
+        rc = self._lib.b200sa_plan_set_weights_device(self.handle, h_cat.data_ptr(),
+                                                      J_cat.data_ptr(), s, err, len(err))
+        _lib.check(rc, err)
+
     def autotune(self, cache_path: str | None = None, force: bool = False) -> list[dict]:
         """Measure launch configurations per size bucket and keep the fastest
         for persistent / graph runs (results are unchanged).  Choices are

@@ -124,6 +124,32 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
     }
     out.max_degree = maxdeg;
     out.any_dup = any_dup;
+    // Back-neighbour records.  Resolution pays when later lanes of a window
+    // often depend on earlier ones: on average at least one back neighbour in
+    // four variables, and no list naming a target twice (the in-register
+    // corrections add one term per neighbour).
+    out.back.assign((size_t)n * 2, 0u);
+    out.bw.clear();
+    out.bw_src.clear();
+    for (int32_t v = 0; v < n; ++v) {
+        uint32_t mask = 0;
+        int32_t at[32];
+        for (int32_t e = out.row[v]; e < out.row[v + 1]; ++e) {
+            const int32_t o = v - out.col[e];
+            if (o > 0 && o < 32) {
+                mask |= 1u << o;
+                at[o] = e;
+            }
+        }
+        out.back[2 * (size_t)v] = mask;
+        out.back[2 * (size_t)v + 1] = (uint32_t)out.bw.size();
+        for (int o = 31; o >= 1; --o) {
+            if (!((mask >> o) & 1u)) continue;
+            out.bw.push_back(out.w[(size_t)at[o]]);
+            out.bw_src.push_back(at[o]);
+        }
+    }
+    out.resolve = !any_dup && n > 0 && 4 * out.bw.size() >= (size_t)n;
     out.regular_degree = 0;
     if (n > 0 && maxdeg > 0 && maxdeg <= 32) {
         bool reg = true;

@@ -18,6 +18,14 @@ struct PackedAdjacency {
     int32_t max_degree = 0;
     int32_t regular_degree = 0;   // common list length when all lists are equally long
     bool any_dup = false;         // some list names a target twice (self-loop / repeat)
+    // In-window resolution (ProblemDev::back, ProblemDev::bw): per variable v
+    // {mask of offsets o in 1..31 with v - o a neighbour, start in bw}; bw the
+    // couplings of those neighbours, nearest-last (offsets descending), and
+    // bw_src the adjacency entry each coupling comes from.
+    std::vector<uint32_t> back;   // 2n
+    std::vector<double> bw;
+    std::vector<int32_t> bw_src;
+    bool resolve = false;         // in-window resolution enabled (ProblemDev::resolve)
 };
 
 // Validates one problem's arguments (lengths, indices, enums, degree limit).

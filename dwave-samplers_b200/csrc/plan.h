@@ -83,13 +83,16 @@ inline void reset_stats(b200sa_stats *s) {
 // Nibble tables of the RNG jump by kHalf outputs (computed once per process).
 const uint32_t (*jump_table())[4];
 
+// Whether plans enable in-window resolution for the problems that qualify.
+bool resolve_allowed();
+
 // Buckets of the persistent mode: a size class crossed with the kernel kind
 // (acceptance rule x update order).  Each bucket's warps get a shared region
 // sized for the bucket's largest n, so small problems pack more resident
 // warps per SM; the last size class keeps its state in global memory.
 constexpr int kSizeClasses = 8;
 constexpr int kGlobalClass = kSizeClasses - 1;
-constexpr int kKinds = 4;
+constexpr int kKinds = kNumKinds;
 constexpr int kBuckets = kSizeClasses * kKinds;
 constexpr int kStreams = 8;
 constexpr int kClassBound[kSizeClasses - 2] = {128, 256, 512, 1024, 2048, 4096};
@@ -101,9 +104,11 @@ inline int size_class(int n, int onchip_max) {
     return kSizeClasses - 2;
 }
 
-// Kernel kind of a problem: bit 0 Gibbs, bit 1 random order.
+// Kernel kind of a problem: bit 0 Gibbs, bit 1 random order, bit 2
+// in-window resolution (sequential order only).
 inline int kind_of(const ProblemDev &d) {
-    return (d.proposal == 0 ? 1 : 0) | (d.varorder ? 2 : 0);
+    return (d.proposal == 0 ? kKindGibbs : 0) | (d.varorder ? kKindRandom : 0) |
+           (d.resolve && !d.varorder ? kKindResolve : 0);
 }
 
 // Launch configuration of one bucket chosen by the autotuner (unset: the
@@ -128,7 +133,7 @@ struct LaunchShape {
 
 // Arena byte offsets of one packed problem.
 struct ArenaOffsets {
-    size_t vinfo, dist, share, col, w, h, cu, cv, cw, betas, thr;
+    size_t vinfo, dist, share, col, w, h, cu, cv, cw, betas, thr, back, bw;
 };
 
 }  // namespace host
@@ -166,6 +171,13 @@ struct b200sa_plan_s {
     int64_t launches = 0;  // sweep-kernel launches issued by the current run
     std::vector<b200sa::host::ArenaOffsets> offs;  // per problem
     std::vector<std::vector<int32_t>> rows;        // per problem: CSR list starts (n + 1)
+    std::vector<std::vector<int32_t>> bw_src;      // per problem: adjacency entry of each bw
+    // Scatter map of b200sa_plan_set_weights_device (built on first use):
+    // arena element sw_dst[i] <- J_cat[sw_src[i]] for i < sw_num_j, else
+    // h_cat[sw_src[i]].
+    b200sa::host::DevArray<int64_t> sw_dst;
+    b200sa::host::DevArray<int32_t> sw_src;
+    int64_t sw_num_j = 0, sw_total = -1;
     b200sa::host::TuneChoice tune[b200sa::host::kBuckets];
     // Persistent launches captured as one CUDA graph, valid for the buffers in
     // graph_key (states in, states out, energies, seeds).

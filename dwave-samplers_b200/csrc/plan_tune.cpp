@@ -304,13 +304,99 @@ int b200sa_plan_set_weights(b200sa_plan plan, int32_t problem, const double *h, 
     B200SA_CUDA(cudaStreamWaitEvent(plan->stream, plan->ev1, 0));
     if (n) B200SA_CUDA(cudaMemcpyAsync(base + o.h, h, 8 * (size_t)n, cudaMemcpyHostToDevice,
                                        plan->stream));
+    // The back-neighbour couplings of the in-window resolution are copies of
+    // adjacency entries.
+    const std::vector<int32_t> &src = plan->bw_src[problem];
+    std::vector<double> bw(src.size());
+    for (size_t i = 0; i < src.size(); ++i) bw[i] = w[(size_t)src[i]];
     if (m) {
         B200SA_CUDA(cudaMemcpyAsync(base + o.w, w.data(), 8 * (size_t)(2 * m),
                                     cudaMemcpyHostToDevice, plan->stream));
         B200SA_CUDA(cudaMemcpyAsync(base + o.cw, J, 8 * (size_t)m, cudaMemcpyHostToDevice,
                                     plan->stream));
     }
+    if (!bw.empty())
+        B200SA_CUDA(cudaMemcpyAsync(base + o.bw, bw.data(), 8 * bw.size(),
+                                    cudaMemcpyHostToDevice, plan->stream));
     B200SA_CUDA(cudaStreamSynchronize(plan->stream));
+    return B200SA_OK;
+}
+
+int b200sa_plan_set_weights_device(b200sa_plan plan, const double *d_h, const double *d_J,
+                                   void *stream, char *err, size_t errlen) {
+    if (!plan) return set_err(err, errlen, B200SA_EINVAL, "plan is NULL");
+    int64_t total_n = 0, total_m = 0;
+    for (int i = 0; i < plan->num_problems; ++i) {
+        total_n += plan->hprobs[i].n;
+        total_m += plan->hprobs[i].m;
+    }
+    if ((total_n > 0 && !d_h) || (total_m > 0 && !d_J))
+        return set_err(err, errlen, B200SA_EINVAL, "h or J is NULL");
+    if (total_n + total_m > (int64_t)INT32_MAX)
+        return set_err(err, errlen, B200SA_EINVAL, "too many fields and couplers");
+    DeviceGuard guard;
+    B200SA_CUDA(cudaSetDevice(plan->device));
+    if (plan->sw_total < 0) {
+        // Each coupler's weight goes to its two adjacency entries (the
+        // packer's fill order, cpu_sa.cpp:298-316, replayed from the list
+        // starts), to its COO copy and to the back-neighbour copies of those
+        // entries; each field to its slot.
+        std::vector<int64_t> dst;
+        std::vector<int32_t> src;
+        std::vector<int64_t> hdst;
+        std::vector<int32_t> hsrc;
+        int64_t joff = 0, hoff = 0;
+        for (int i = 0; i < plan->num_problems; ++i) {
+            const ProblemDev &d = plan->hprobs[i];
+            const ArenaOffsets &o = plan->offs[i];
+            const int64_t m = d.m;
+            std::vector<int32_t> hcu((size_t)m), hcv((size_t)m), coupler((size_t)(2 * m));
+            if (m) {
+                B200SA_CUDA(cudaMemcpy(hcu.data(), d.cu, 4 * (size_t)m, cudaMemcpyDeviceToHost));
+                B200SA_CUDA(cudaMemcpy(hcv.data(), d.cv, 4 * (size_t)m, cudaMemcpyDeviceToHost));
+            }
+            const std::vector<int32_t> &row = plan->rows[i];
+            std::vector<int32_t> cur(row.begin(), row.end() - 1);
+            for (int64_t c = 0; c < m; ++c) {
+                const int32_t eu = cur[hcu[c]]++, ev = cur[hcv[c]]++;
+                coupler[(size_t)eu] = (int32_t)c;
+                coupler[(size_t)ev] = (int32_t)c;
+                dst.push_back((int64_t)(o.w / 8) + eu);
+                src.push_back((int32_t)(joff + c));
+                dst.push_back((int64_t)(o.w / 8) + ev);
+                src.push_back((int32_t)(joff + c));
+                dst.push_back((int64_t)(o.cw / 8) + c);
+                src.push_back((int32_t)(joff + c));
+            }
+            const std::vector<int32_t> &bs = plan->bw_src[i];
+            for (size_t k = 0; k < bs.size(); ++k) {
+                dst.push_back((int64_t)(o.bw / 8) + (int64_t)k);
+                src.push_back((int32_t)(joff + coupler[(size_t)bs[k]]));
+            }
+            for (int32_t v = 0; v < d.n; ++v) {
+                hdst.push_back((int64_t)(o.h / 8) + v);
+                hsrc.push_back((int32_t)(hoff + v));
+            }
+            joff += m;
+            hoff += d.n;
+        }
+        const int64_t num_j = (int64_t)dst.size();
+        dst.insert(dst.end(), hdst.begin(), hdst.end());
+        src.insert(src.end(), hsrc.begin(), hsrc.end());
+        B200SA_CUDA(plan->sw_dst.alloc(std::max<size_t>(dst.size(), 1)));
+        B200SA_CUDA(plan->sw_src.alloc(std::max<size_t>(src.size(), 1)));
+        if (!dst.empty()) {
+            B200SA_CUDA(cudaMemcpy(plan->sw_dst.ptr, dst.data(), 8 * dst.size(),
+                                   cudaMemcpyHostToDevice));
+            B200SA_CUDA(cudaMemcpy(plan->sw_src.ptr, src.data(), 4 * src.size(),
+                                   cudaMemcpyHostToDevice));
+        }
+        plan->sw_num_j = num_j;
+        plan->sw_total = (int64_t)dst.size();
+    }
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : plan->stream;
+    B200SA_CUDA(scatter_weights(reinterpret_cast<double *>(plan->arena.ptr), plan->sw_dst.ptr,
+                                plan->sw_src.ptr, plan->sw_num_j, plan->sw_total, d_J, d_h, st));
     return B200SA_OK;
 }
 
@@ -357,7 +443,7 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
                 if (stage == kStageShared && max_n > plan->onchip_max) continue;
                 const int region = region_bytes_for_stage(stage, stage == kStageGlobal ? 0 : max_n);
                 if (region > smem_blk) continue;
-                const int variant = kernel_variant(kind & 1, kind & 2, stage, regs);
+                const int variant = kernel_variant(kind, stage, regs);
                 int resident[kMaxThreadsPerCta / 32 + 1] = {};
                 int ctas_of[kMaxThreadsPerCta / 32 + 1] = {};
                 int top = 0;
@@ -383,6 +469,28 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
                     TuneChoice c = cands.back();
                     c.ctas_per_sm = ctas_of[widest] - 1;
                     cands.push_back(c);
+                }
+                // State in global slots: fewer resident warps also means
+                // fewer slots competing for L2 (delta energies, 8 bytes a
+                // variable, and spins for the global location).  Offer the
+                // widest CTA with its CTAs per SM capped so that the slots
+                // fit in 40% and in 70% of L2.
+                if (widest && stage != kStageShared) {
+                    const double per_warp = (double)max_n * (stage == kStageGlobal ? 9.0 : 8.0);
+                    const double l2 = (double)plan->prop.l2CacheSize;
+                    int last_cap = ctas_of[widest] - 1;
+                    for (double share : {0.7, 0.4}) {
+                        const int cap = (int)(share * l2 / (per_warp * sms * widest));
+                        if (cap < 1 || cap >= last_cap) continue;
+                        TuneChoice c;
+                        c.set = true;
+                        c.staging = stage;
+                        c.warps_per_cta = widest;
+                        c.reg_class = regs;
+                        c.ctas_per_sm = cap;
+                        cands.push_back(c);
+                        last_cap = cap;
+                    }
                 }
             }
             float best_ms = 0.f;

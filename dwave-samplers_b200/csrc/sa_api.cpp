@@ -49,6 +49,16 @@ int select_device(int device, cudaDeviceProp &prop, char *err, size_t errlen) {
 }
 
 
+// In-window resolution of the sequential sweep is on unless the environment
+// sets B200SA_RESOLVE=0 (results are identical either way; for A/B timing).
+bool resolve_allowed() {
+    static const bool on = [] {
+        const char *e = std::getenv("B200SA_RESOLVE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 const uint32_t (*jump_table())[4] {
     static uint32_t table[kJumpTable][4];
     static std::once_flag once;
@@ -88,7 +98,7 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
     const int cap = stage == kStageGlobal ? 0 : max_n_here;
     const int region = region_bytes_for_stage(stage, cap);
     const int reg_class = choice && choice->set ? choice->reg_class : 0;
-    const int variant = kernel_variant(kind & 1, kind & 2, stage, reg_class);
+    const int variant = kernel_variant(kind, stage, reg_class);
     out.stage = stage;
     if (choice && choice->set) {
         // The autotuner's measured configuration (a persistent launch takes
@@ -412,6 +422,8 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         o.cw = take(8 * m);
         o.betas = take(8 * nb);
         o.thr = take(8 * nb);
+        o.back = take(8 * n);
+        o.bw = take(8 * adj[i].bw.size());
         P->state_off[i + 1] = P->state_off[i] + (int64_t)q.num_reads * q.num_vars;
         P->read_off[i + 1] = P->read_off[i] + q.num_reads;
         P->n.push_back(q.num_vars);
@@ -439,7 +451,10 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
             std::memcpy(&staging[o.dist], adj[i].dist.data(), n);
             std::memcpy(&staging[o.share], adj[i].share.data(), 4 * n);
             std::memcpy(&staging[o.h], q.h, 8 * n);
+            std::memcpy(&staging[o.back], adj[i].back.data(), 8 * n);
         }
+        if (!adj[i].bw.empty())
+            std::memcpy(&staging[o.bw], adj[i].bw.data(), 8 * adj[i].bw.size());
         if (nb) {
             std::memcpy(&staging[o.betas], q.beta_schedule, 8 * nb);
             double *thr = reinterpret_cast<double *>(&staging[o.thr]);
@@ -453,6 +468,7 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
                                     cudaMemcpyHostToDevice, P->stream));
     P->offs = off;
     P->rows.resize((size_t)num_problems);
+    P->bw_src.resize((size_t)num_problems);
     for (int32_t i = 0; i < num_problems; ++i) P->rows[i] = std::move(adj[i].row);
     P->hprobs.resize((size_t)num_problems);
     for (int32_t i = 0; i < num_problems; ++i) {
@@ -484,6 +500,11 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         d.regular_magic = d.regular_degree ? (65536u + (uint32_t)d.regular_degree - 1) /
                                                  (uint32_t)d.regular_degree
                                            : 0u;
+        d.resolve = (adj[i].resolve && resolve_allowed()) ? 1 : 0;
+        d.pad_ = 0;
+        d.back = reinterpret_cast<const uint2 *>(base + o.back);
+        d.bw = reinterpret_cast<const double *>(base + o.bw);
+        P->bw_src[i] = std::move(adj[i].bw_src);
     }
     B200SA_CUDA(P->dprobs.alloc((size_t)std::max(num_problems, 1)));
     if (num_problems)
@@ -871,7 +892,8 @@ int b200sa_plan_bucket_report(b200sa_plan plan, b200sa_bucket_report *out, int32
                 r.staging = s.stage;
                 r.warps_per_cta = s.warps_per_cta;
                 r.grid = s.grid;
-                r.registers = (s.variant >> 4) == 1 ? kRegs80 : (s.variant >> 4) == 2 ? kRegs64 : 128;
+                const int rc = variant_reg_class(s.variant);
+                r.registers = rc == 1 ? kRegs80 : rc == 2 ? kRegs64 : 128;
             }
         }
         ++k;

@@ -144,6 +144,8 @@ struct Prob {
     const uint32_t *__restrict__ share;
     int regular_degree;
     uint32_t regular_magic;
+    const uint2 *__restrict__ back;
+    const double *__restrict__ bw;
 };
 
 __device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
@@ -160,6 +162,8 @@ __device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
     q.share = P->share;
     q.regular_degree = P->regular_degree;
     q.regular_magic = P->regular_magic;
+    q.back = P->back;
+    q.bw = P->bw;
     return q;
 }
 
@@ -249,7 +253,8 @@ __device__ __forceinline__ void ring_refill(uint64_t *ring, RingState &rs,
 }
 
 // cpu_sa.cpp:54-74 for every variable, then the working copy of the spins.
-__device__ __forceinline__ void load_state(const ProblemDev *PD, const int8_t *src,
+// Returns (warp-uniform) whether every spin is +1 or -1.
+__device__ __forceinline__ bool load_state(const ProblemDev *PD, const int8_t *src,
                                            double *de, int8_t *sp,
                                            unsigned lane) {
     const int n = PD->n;
@@ -257,7 +262,13 @@ __device__ __forceinline__ void load_state(const ProblemDev *PD, const int8_t *s
     const int32_t *__restrict__ col = PD->col;
     const double *__restrict__ w = PD->w;
     const double *__restrict__ h = PD->h;
-    for (int v = lane; v < n; v += 32) sp[v] = src[v];
+    bool pm1 = true;
+    for (int v = lane; v < n; v += 32) {
+        const int8_t x = src[v];
+        sp[v] = x;
+        pm1 = pm1 && (x == 1 || x == -1);
+    }
+    pm1 = __all_sync(kFull, pm1);
     __syncwarp();
     for (int v = lane; v < n; v += 32) {
         const uint2 vi = __ldg(&vinfo[v]);
@@ -268,6 +279,7 @@ __device__ __forceinline__ void load_state(const ProblemDev *PD, const int8_t *s
         de[v] = __dmul_rn((double)(-2 * (int)sp[v]), f);
     }
     __syncwarp();
+    return pm1;
 }
 
 // cpu_sa.cpp:168-191 for every lane whose bit is set in `fm`.  Lane k of
@@ -355,16 +367,17 @@ __device__ __forceinline__ void apply_flips(const Prob &P, double *de, int8_t *s
 // Neighbour updates of the committed flips for equal-length lists (D entries
 // each, list v at v * D).  `rank_tab[f]` is the lane of the f-th committed
 // flip in variable order; `mult` is each lane's (int8)(4 * s) as a double
-// (cpu_sa.cpp:172), read by the entry's owner lane.  The entries of the first
-// 64 accepted flips were loaded into (nb0, w0, k0) / (nb1, w1, k1) before the
-// commit point was known (the committed flips are a prefix of the accepted
-// ones); later entries are loaded here.  Equal targets within a round are
-// summed in entry order by their first lane, as in apply_flips.
+// (cpu_sa.cpp:172), read by the entry's owner lane.  With `pre`, the entries
+// of the first 64 accepted flips were loaded into (nb0, w0, k0) / (nb1, w1,
+// k1) before the commit point was known (the committed flips are then a
+// prefix of the accepted ones); the other entries are loaded here.  Equal
+// targets within a round are summed in entry order by their first lane, as in
+// apply_flips.
 __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t *sp,
                                                double *scratch, const int *rank_tab,
-                                               int nflips, int p, int nb0, double w0, int k0,
-                                               int nb1, double w1, int k1, bool may_conflict,
-                                               double mult, unsigned lane) {
+                                               int nflips, int p, bool pre, int nb0, double w0,
+                                               int k0, int nb1, double w1, int k1,
+                                               bool may_conflict, double mult, unsigned lane) {
     const int D = P.regular_degree;
     const int total = nflips * D;
     for (int base = 0; base < total; base += 32) {
@@ -372,9 +385,9 @@ __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t
         const bool a = t < total;
         int k, nb;
         double wt;
-        if (base == 0) {
+        if (pre && base == 0) {
             k = k0, nb = nb0, wt = w0;
-        } else if (base == 32) {
+        } else if (pre && base == 32) {
             k = k1, nb = nb1, wt = w1;
         } else {
             k = 0, nb = 0, wt = 0.0;
@@ -414,17 +427,44 @@ __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t
     }
 }
 
+// One acceptance decision (cpu_sa.cpp:144-166) for a lane that needs a draw:
+// the single-precision bounds first, the exact double test inside the band.
+// Returns accept in bit 0 and the near-tie flag in bit 1.
+template <bool GIBBS>
+__device__ __forceinline__ int decide(double d, double beta, uint64_t r) {
+    const int fast = GIBBS ? gibbs_fast(__dmul_rn(d, beta), r)
+                           : metropolis_fast(__dmul_rn(-d, beta), r);
+    if (fast >= 0) return fast;
+    return GIBBS ? gibbs_exact(d, beta, r) : metropolis_exact(d, beta, r);
+}
+
 // Sequential order (cpu_sa.cpp:132-192) in speculative passes over windows
 // of 32 consecutive variables, one per lane.  Every lane decides its variable
-// against the delta energies at the start of the pass; the pass commits the
-// prefix of the window that ends before the first variable whose decision a
-// committed flip could have changed (a later neighbour of an accepted flip),
-// so the committed decisions equal the sequential ones.
+// against the delta energies at the start of the pass; the first round
+// commits the prefix of the window that ends before the first variable whose
+// decision a committed flip could have changed (a later neighbour of an
+// accepted flip), so the committed decisions equal the sequential ones.
+//
+// With `resolve` (problems whose lists name no target twice, reads whose
+// spins are all +-1) the pass goes on in further rounds instead of ending
+// there.  The flips committed by a round add their contributions
+// ((4 s_j) J) s_k (cpu_sa.cpp:172-185) to the delta energies, held in
+// registers, of the uncommitted lanes they neighbour, in variable order as the
+// reference adds them; those lanes decide again, their draws placed after the
+// ones already committed, and the next commit point follows by the same rule.
+// Each round commits at least its first lane.  The update phase then applies
+// every committed flip's entries to the delta energies in memory in entry
+// order with the spins as they were at the start of the pass, and negates the
+// flipped variables' own delta energies last: negation is exact and commutes
+// with rounding, so a contribution added after the negation in the reference
+// (a neighbour that flipped earlier) equals the negated contribution added
+// before it.
 template <bool GIBBS>
 __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                                                  int8_t *sp, double *scratch,
                                                  uint64_t *ring, RingState &rs,
-                                                 unsigned lane, Counters &cnt) {
+                                                 unsigned lane, Counters &cnt,
+                                                 bool resolve) {
     const int n = P.n;
     const int D = P.regular_degree;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -443,11 +483,17 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                 int dist = (int)kDistCap;
                 uint32_t shr = 0u;
                 uint2 vi = make_uint2(0u, 0u);
+                uint2 bk = make_uint2(0u, 0u);
+                int s_cur = 0;
                 if (act) {
                     d = de[v];
                     dist = __ldg(&P.dist[v]);
                     shr = __ldg(&P.share[v]);
                     if (!D) vi = __ldg(&P.vinfo[v]);
+                    if (resolve) {
+                        bk = __ldg(&P.back[v]);
+                        s_cur = (int)sp[v];
+                    }
                 }
                 const bool consider = act && !(d >= thr);  // cpu_sa.cpp:140
                 const bool need = GIBBS ? consider : (consider && !(d <= 0.0));
@@ -456,33 +502,29 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                 bool near = false;
                 if (need) {
                     const uint64_t r = ring[(rs.q + (uint32_t)__popc(nm & lt_mask)) & (kRing - 1)];
-                    const int fast = GIBBS ? gibbs_fast(__dmul_rn(d, beta), r)
-                                           : metropolis_fast(__dmul_rn(-d, beta), r);
-                    if (fast >= 0) {
-                        acc = fast != 0;
-                    } else {
-                        const int ex = GIBBS ? gibbs_exact(d, beta, r) : metropolis_exact(d, beta, r);
-                        acc = (ex & 1) != 0;
-                        near = (ex & 2) != 0;
-                    }
+                    const int x = decide<GIBBS>(d, beta, r);
+                    acc = (x & 1) != 0;
+                    near = (x & 2) != 0;
                 }
                 const unsigned am = __ballot_sync(kFull, acc);
                 // Equal-length lists: start loading the accepted flips'
-                // adjacency before the commit point is known.
+                // adjacency before the commit point is known (not with
+                // resolution, whose later rounds change the accepted set).
+                const bool pre = !resolve;
                 int nb0 = 0, nb1 = 0, k0 = 0, k1 = 0;
                 double w0 = 0.0, w1 = 0.0;
-                if (D && am) {
+                if (D && am && pre) {
                     if (acc) rank_tab[__popc(am & lt_mask)] = (int)lane;
                     __syncwarp();
-                    const int pre = min(__popc(am) * D, 64);
-                    if ((int)lane < pre) {
+                    const int pre_n = min(__popc(am) * D, 64);
+                    if ((int)lane < pre_n) {
                         const int r = (int)((lane * P.regular_magic) >> 16);
                         k0 = rank_tab[r];
                         const int e = (p + k0) * D + ((int)lane - r * D);
                         nb0 = __ldg(&P.col[e]);
                         w0 = __ldg(&P.w[e]);
                     }
-                    if ((int)lane + 32 < pre) {
+                    if ((int)lane + 32 < pre_n) {
                         const int t = (int)lane + 32;
                         const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
                         k1 = rank_tab[r];
@@ -492,15 +534,63 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                     }
                 }
                 const int bound = acc ? (int)lane + dist : 32;
-                const int c = min(__reduce_min_sync(kFull, bound), L);
-                const unsigned commit = c >= 32 ? kFull : ((1u << c) - 1u);
-                rs.q += (uint32_t)__popc(nm & commit);
-                const unsigned fm = am & commit;
-                cnt.near += __popc(__ballot_sync(kFull, near) & commit);
+                int c = min(__reduce_min_sync(kFull, bound), L);
+                unsigned done = c >= 32 ? kFull : ((1u << c) - 1u);
+                uint32_t used = (uint32_t)__popc(nm & done);
+                unsigned fm = am & done;
+                unsigned nearm = __ballot_sync(kFull, near) & done;
+                if (resolve && c < L) {
+                    // Lanes j < lane whose variables neighbour this lane's.
+                    const unsigned back_lanes = __brev(bk.x) >> (31u - lane);
+                    const unsigned smask = __ballot_sync(kFull, s_cur > 0);
+                    const double sk = (double)s_cur;
+                    unsigned newf = fm;
+                    do {
+                        if (act && (int)lane >= c) {
+                            unsigned rel = back_lanes & newf;
+                            while (rel) {
+                                const int j = __ffs(rel) - 1;
+                                rel &= rel - 1u;
+                                const int o = (int)lane - j;
+                                // Offsets are stored descending: o's rank
+                                // is the number of larger offsets.
+                                const int rank = __popcll((unsigned long long)bk.x >> (o + 1));
+                                const double wj = __ldg(&P.bw[bk.y + (uint32_t)rank]);
+                                const double mj = ((smask >> j) & 1u) ? 4.0 : -4.0;
+                                d = __dadd_rn(d, __dmul_rn(__dmul_rn(mj, wj), sk));
+                            }
+                        }
+                        const bool live = act && (int)lane >= c;
+                        const bool cons2 = live && !(d >= thr);
+                        const bool need2 = GIBBS ? cons2 : (cons2 && !(d <= 0.0));
+                        const unsigned nm2 = __ballot_sync(kFull, need2);
+                        bool acc2 = GIBBS ? false : cons2;
+                        bool near2 = false;
+                        if (need2) {
+                            const uint64_t r =
+                                ring[(rs.q + used + (uint32_t)__popc(nm2 & lt_mask)) & (kRing - 1)];
+                            const int x = decide<GIBBS>(d, beta, r);
+                            acc2 = (x & 1) != 0;
+                            near2 = (x & 2) != 0;
+                        }
+                        const unsigned am2 = __ballot_sync(kFull, acc2);
+                        const int bound2 = acc2 ? (int)lane + dist : 32;
+                        c = min(__reduce_min_sync(kFull, bound2), L);
+                        const unsigned upto = c >= 32 ? kFull : ((1u << c) - 1u);
+                        const unsigned commit2 = upto & ~done;
+                        used += (uint32_t)__popc(nm2 & commit2);
+                        nearm |= __ballot_sync(kFull, near2) & commit2;
+                        newf = am2 & commit2;
+                        fm |= newf;
+                        done = upto;
+                    } while (c < L);
+                }
+                rs.q += used;
+                cnt.near += __popc(nearm);
                 cnt.flips += __popc(fm);
                 cnt.passes += 1;
                 if (fm) {
-                    const int s_cur = act ? (int)sp[v] : 0;
+                    if (!resolve) s_cur = act ? (int)sp[v] : 0;
                     // A slot can receive two additions only through a repeated
                     // target in one list or a neighbour common to two flips.
                     const unsigned later = lane < 31 ? fm >> (lane + 1) : 0u;
@@ -508,8 +598,12 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                     const bool may_conflict =
                         __any_sync(kFull, f && ((shr & 1u) || ((shr >> 1) & later)));
                     if (D) {
-                        update_regular(P, de, sp, scratch, rank_tab, __popc(fm), p, nb0, w0, k0,
-                                       nb1, w1, k1, may_conflict,
+                        if (!pre) {
+                            if (f) rank_tab[__popc(fm & lt_mask)] = (int)lane;
+                            __syncwarp();
+                        }
+                        update_regular(P, de, sp, scratch, rank_tab, __popc(fm), p, pre, nb0, w0,
+                                       k0, nb1, w1, k1, may_conflict,
                                        (double)(int)(int8_t)(4 * s_cur), lane);
                         if (f) {  // cpu_sa.cpp:189-190, after the variable's own updates
                             sp[v] = (int8_t)(-s_cur);
@@ -607,20 +701,20 @@ __device__ __forceinline__ double state_energy(const ProblemDev *PD, const int8_
     return e;
 }
 
-template <bool GIBBS, bool RANDOM_ORDER>
+template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE>
 __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *src,
                                             int8_t *dst, double *energy_out,
                                             double *de, int8_t *sp,
                                             double *scratch, uint64_t *ring,
                                             RingState &rs, unsigned lane,
                                             Counters &cnt) {
-    load_state(PD, src, de, sp, lane);
+    const bool pm1 = load_state(PD, src, de, sp, lane);
     {
         const Prob P = load_prob(PD);
         if (RANDOM_ORDER)
             sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
         else
-            sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
+            sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, RESOLVE && pm1);
     }
     __syncwarp();
     const double e = state_energy(PD, sp, lane);

@@ -8,6 +8,8 @@
 // has enough reads to fill them; the autotuner chooses per bucket.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "sa_kernel.cuh"
 #include "sa_launch.h"
 #include "sd_kernel.cuh"
@@ -16,7 +18,7 @@
 
 namespace b200sa {
 
-template <bool GIBBS, bool RANDOM_ORDER, int STAGE>
+template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE, int STAGE>
 __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_cta,
                                              int region_bytes) {
     extern __shared__ __align__(16) uint8_t smem[];
@@ -73,7 +75,7 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
         }
         const int64_t so = PD->state_offset + (int64_t)r * PD->n;
         Counters cnt = {0ull, 0ull, 0u};
-        anneal_read<GIBBS, RANDOM_ORDER>(PD, A.states_in + so, A.states_out + so,
+        anneal_read<GIBBS, RANDOM_ORDER, RESOLVE>(PD, A.states_in + so, A.states_out + so,
                                             &A.energies[rd], de, sp, scratch, ring, rs, lane,
                                             cnt);
         if (lane == 0) {
@@ -96,40 +98,44 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
     }
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, int STAGE>
+template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE, int STAGE>
 __global__ void __launch_bounds__(kMaxThreadsPerCta, 1)
     sa_warp_kernel(LaunchArgs A, int warps_per_cta, int region_bytes) {
-    sa_warp_body<GIBBS, RANDOM_ORDER, STAGE>(A, warps_per_cta, region_bytes);
+    sa_warp_body<GIBBS, RANDOM_ORDER, RESOLVE, STAGE>(A, warps_per_cta, region_bytes);
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, int STAGE>
+template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE, int STAGE>
 __global__ void __maxnreg__(kRegs80) sa_warp_kernel_r80(LaunchArgs A, int warps_per_cta,
                                                          int region_bytes) {
-    sa_warp_body<GIBBS, RANDOM_ORDER, STAGE>(A, warps_per_cta, region_bytes);
+    sa_warp_body<GIBBS, RANDOM_ORDER, RESOLVE, STAGE>(A, warps_per_cta, region_bytes);
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, int STAGE>
+template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE, int STAGE>
 __global__ void __maxnreg__(kRegs64) sa_warp_kernel_r64(LaunchArgs A, int warps_per_cta,
                                                          int region_bytes) {
-    sa_warp_body<GIBBS, RANDOM_ORDER, STAGE>(A, warps_per_cta, region_bytes);
+    sa_warp_body<GIBBS, RANDOM_ORDER, RESOLVE, STAGE>(A, warps_per_cta, region_bytes);
 }
 
 using KernelFn = void (*)(LaunchArgs, int, int);
 
-#define B200SA_KINDS(name, stage)                                                     \
-    name<false, false, stage>, name<true, false, stage>, name<false, true, stage>,   \
-        name<true, true, stage>
-#define B200SA_KERNEL_TABLE(name)                                                     \
-    {B200SA_KINDS(name, kStageGlobal), B200SA_KINDS(name, kStageShared),             \
+// Kinds in the order of their numbers (bit 0 Gibbs, bit 1 random order,
+// bit 2 in-window resolution); resolution exists for sequential order only.
+#define B200SA_KINDS(name, stage)                                                      \
+    name<false, false, false, stage>, name<true, false, false, stage>,                 \
+        name<false, true, false, stage>, name<true, true, false, stage>,               \
+        name<false, false, true, stage>, name<true, false, true, stage>, nullptr, nullptr
+#define B200SA_KERNEL_TABLE(name)                                                      \
+    {B200SA_KINDS(name, kStageGlobal), B200SA_KINDS(name, kStageShared),              \
      B200SA_KINDS(name, kStageSpins)}
 
 static KernelFn kernel_for(int variant) {
-    static const KernelFn k128[12] = B200SA_KERNEL_TABLE(sa_warp_kernel);
-    static const KernelFn k80[12] = B200SA_KERNEL_TABLE(sa_warp_kernel_r80);
-    static const KernelFn k64[12] = B200SA_KERNEL_TABLE(sa_warp_kernel_r64);
-    const int idx = variant & 15;  // kind (bits 0-1) and state location (bits 2-3)
-    if (idx >= 12) return nullptr;
-    switch (variant >> 4) {
+    constexpr int kPerClass = 3 * kNumKinds;
+    static const KernelFn k128[kPerClass] = B200SA_KERNEL_TABLE(sa_warp_kernel);
+    static const KernelFn k80[kPerClass] = B200SA_KERNEL_TABLE(sa_warp_kernel_r80);
+    static const KernelFn k64[kPerClass] = B200SA_KERNEL_TABLE(sa_warp_kernel_r64);
+    const int idx = variant & 31;  // kind (bits 0-2) and state location (bits 3-4)
+    if (idx >= kPerClass) return nullptr;
+    switch (variant_reg_class(variant)) {
         case 0: return k128[idx];
         case 1: return k80[idx];
         case 2: return k64[idx];
@@ -194,6 +200,26 @@ __global__ void acceptance_check_kernel(int64_t samples, uint64_t seed,
 
 cudaError_t acceptance_check(int64_t samples, uint64_t seed, unsigned long long *d_counts) {
     acceptance_check_kernel<<<148 * 4, 256>>>(samples, seed, d_counts);
+    return cudaGetLastError();
+}
+
+// arena[dst[i]] = (i < num_j ? J[src[i]] : h[src[i]]): the coupler weights
+// (adjacency entries, COO copy, back-neighbour copies) and the fields of
+// every problem of a plan, from the concatenated inputs.
+__global__ void scatter_weights_kernel(double *arena, const int64_t *dst, const int32_t *src,
+                                       int64_t num_j, int64_t total, const double *J,
+                                       const double *h) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x)
+        arena[dst[i]] = i < num_j ? J[src[i]] : h[src[i]];
+}
+
+cudaError_t scatter_weights(double *arena, const int64_t *dst, const int32_t *src, int64_t num_j,
+                            int64_t total, const double *J, const double *h,
+                            cudaStream_t stream) {
+    if (total <= 0) return cudaSuccess;
+    const int64_t blocks = std::min<int64_t>((total + 255) / 256, 148 * 8);
+    scatter_weights_kernel<<<(int)blocks, 256, 0, stream>>>(arena, dst, src, num_j, total, J, h);
     return cudaGetLastError();
 }
 

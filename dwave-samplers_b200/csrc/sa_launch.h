@@ -15,14 +15,25 @@ constexpr int kRegs80 = 80;
 constexpr int kRegs64 = 64;
 constexpr int kRegClasses = 3;  // 0: 128, 1: 80, 2: 64
 
-// Kernel variant: bit 0 Gibbs, bit 1 random order, bits 2-3 state location
-// (kStageGlobal, kStageShared, kStageSpins), bits 4-5 register class (0: 128,
-// 1: 80, 2: 64 registers).
-inline int kernel_variant(bool gibbs, bool random_order, int stage, int reg_class = 0) {
-    return (gibbs ? 1 : 0) | (random_order ? 2 : 0) | (stage << 2) | (reg_class << 4);
+// Kernel kind: bit 0 Gibbs, bit 1 random order, bit 2 in-window resolution
+// (sequential order only; ProblemDev::resolve).
+constexpr int kKindGibbs = 1;
+constexpr int kKindRandom = 2;
+constexpr int kKindResolve = 4;
+constexpr int kNumKinds = 8;
+
+// Kernel variant: bits 0-2 kind, bits 3-4 state location (kStageGlobal,
+// kStageShared, kStageSpins), bits 5-6 register class (0: 128, 1: 80, 2: 64
+// registers).
+inline int kernel_variant(int kind, int stage, int reg_class = 0) {
+    return (kind & (kNumKinds - 1)) | (stage << 3) | (reg_class << 5);
 }
+inline int variant_reg_class(int variant) { return variant >> 5; }
 
 cudaError_t upload_jump_table(const uint32_t table[][4], cudaStream_t stream);
+cudaError_t scatter_weights(double *arena, const int64_t *dst, const int32_t *src, int64_t num_j,
+                            int64_t total, const double *J, const double *h,
+                            cudaStream_t stream);
 cudaError_t launch_sa(int variant, const LaunchArgs &args, int grid, int warps_per_cta,
                       int region_bytes, cudaStream_t stream);
 cudaError_t kernel_occupancy(int variant, int warps_per_cta, int region_bytes,

@@ -192,6 +192,10 @@ __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
         P->proposal = a.proposal;
         P->regular_degree = 0;  // general lists
         P->regular_magic = 0;
+        P->resolve = 0;  // no back-neighbour records: passes end at the first dependent
+        P->pad_ = 0;
+        P->back = nullptr;
+        P->bw = nullptr;
     }
 }
 
@@ -365,7 +369,9 @@ extern "C" int b200sa_sample_noalloc(
         return fail(err, errlen, B200SA_EINVAL, "coupler indexes contain an invalid variable");
 
     // Launch shape: every read's state on chip (n <= 4096); most resident warps.
-    const int variant = kernel_variant(proposal == B200SA_GIBBS, varorder == B200SA_RANDOM, true);
+    const int variant = kernel_variant(
+        (proposal == B200SA_GIBBS ? kKindGibbs : 0) | (varorder == B200SA_RANDOM ? kKindRandom : 0),
+        kStageShared);
     const int region = region_bytes_for(num_vars);
     int best_w = 1, best = 0;
     for (int wpc = 1; wpc <= kMaxThreadsPerCta / 32; ++wpc) {

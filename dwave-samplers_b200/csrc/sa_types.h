@@ -58,6 +58,15 @@ struct ProblemDev {
     // v * regular_degree; 0 when the lists differ in length.
     int32_t regular_degree;
     uint32_t regular_magic;  // ceil(2^16 / regular_degree): t / D == (t * magic) >> 16 for t < 1024
+    // In-window resolution of the sequential sweep (1: on, for reads whose
+    // spins are all +-1).  back[v] = {mask, start}: bit o (1..31) of mask set
+    // when v - o is a neighbour of v; bw[start ..] the couplings of those
+    // neighbours, offsets descending (the order the reference adds their
+    // flips' contributions).  No list may name a target twice.
+    int32_t resolve;
+    int32_t pad_;
+    const uint2 *back;
+    const double *bw;
 };
 
 // Per-read counters written by the kernel.

@@ -173,6 +173,20 @@ B200SA_API int b200sa_plan_destroy(b200sa_plan plan);
 B200SA_API int b200sa_plan_set_weights(b200sa_plan plan, int32_t problem, const double *h,
                                        const double *J, char *err, size_t errlen);
 
+/* Device-side form of b200sa_plan_set_weights for every problem of the plan
+ * at once (no reference counterpart): d_h holds the fields of all problems
+ * concatenated (problem after problem, num_vars each) and d_J their coupler
+ * weights (num_couplers each, COO order as at creation), both DEVICE arrays.
+ * The update is enqueued on `stream` (a cudaStream_t; NULL selects the
+ * plan's own stream): runs enqueued before it on that stream see the old
+ * weights, runs after it the new ones; a captured graph stays valid.  The
+ * first call builds the scatter map on the device (it allocates and waits);
+ * later calls launch one kernel and return at once.  Returns 0 or a negative
+ * error. */
+B200SA_API int b200sa_plan_set_weights_device(b200sa_plan plan, const double *d_h,
+                                              const double *d_J, void *stream, char *err,
+                                              size_t errlen);
+
 /* ---- Autotuner (no reference counterpart) ---------------------------------
  * For every non-empty bucket of a plan (size class x acceptance rule x order)
  * times candidate launch configurations -- warps per CTA, CTAs per SM, the
@@ -190,7 +204,7 @@ B200SA_API int b200sa_plan_set_weights(b200sa_plan plan, int32_t problem, const 
 #define B200SA_TUNE_FORCE 1
 typedef struct {
     int32_t bucket;
-    int32_t kind;           /* bit 0 Gibbs, bit 1 random order */
+    int32_t kind;           /* bit 0 Gibbs, bit 1 random order, bit 2 in-window resolution */
     int32_t max_n;
     int64_t items;          /* reads in the bucket */
     int32_t staging;        /* state: 0 global slot (L2), 1 shared memory, 2 spins in
@@ -218,7 +232,7 @@ B200SA_API int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, in
  * non-empty buckets (up to cap entries written) or a negative error. */
 typedef struct {
     int32_t bucket;
-    int32_t kind;           /* bit 0 Gibbs, bit 1 random order */
+    int32_t kind;           /* bit 0 Gibbs, bit 1 random order, bit 2 in-window resolution */
     int32_t max_n;
     int64_t reads;
     int64_t attempts;

@@ -145,6 +145,53 @@ def test_shared_stream_matches_reference_multiread():
     np.testing.assert_array_equal(s2, want_s[:7])
 
 
+# ---- in-window resolution (problems where later lanes depend on earlier) ---
+
+def test_in_window_resolution_is_active_and_exact():
+    """At high temperature nearly every attempt flips.  On the lattice each
+    site neighbours its successor, so a pass that ended at the first
+    dependent lane would commit one or two attempts; with in-window
+    resolution a pass commits the whole window."""
+    inst = workloads.cubic_lattice(L=8, reads=64, sweeps=60, beta_range=(0.02, 0.3), seed=7)
+    stats = {}
+    s, e = simulated_annealing(64, inst.h, inst.u, inst.v, inst.J, 1, inst.betas, 0,
+                               inst.states.copy(), seeds=inst.seeds, stats=stats)
+    assert stats["attempts"] / stats["passes"] > 24
+    assert stats["flips"] > stats["attempts"] // 2
+    ws, we = oracle.run(inst.h, inst.u, inst.v, inst.J, inst.states, 1, inst.betas, inst.seeds)
+    np.testing.assert_array_equal(s, ws)
+    np.testing.assert_array_equal(bits(e), bits(we))
+
+
+@pytest.mark.parametrize("gibbs", [False, True])
+def test_in_window_resolution_shared_stream_and_odd_spins(gibbs):
+    """Dense problem (resolution on): one RNG stream continued across reads,
+    and reads whose spins are not all +-1 (resolution off for those reads,
+    in the same launch as reads that use it)."""
+    rng = np.random.default_rng(21 + gibbs)
+    n = 60
+    iu, ju = np.triu_indices(n, 1)
+    keep = rng.random(iu.shape[0]) < 0.4
+    u, v = iu[keep].astype(np.int32), ju[keep].astype(np.int32)
+    J = rng.uniform(-1, 1, u.shape[0])
+    h = rng.uniform(-1, 1, n)
+    betas = np.geomspace(0.05, 3.0, 60)
+    crit = "Gibbs" if gibbs else "Metropolis"
+    st = (2 * rng.integers(0, 2, (10, n)) - 1).astype(np.int8)
+    want_s, want_e = oracle.run(h, u, v, J, st, 1, betas, [777], False, gibbs)
+    s, e = simulated_annealing(10, h, u, v, J, 1, betas, 777, st.copy(), False, crit,
+                               rng_stream="shared")
+    np.testing.assert_array_equal(s, want_s)
+    np.testing.assert_array_equal(bits(e), bits(want_e))
+    st[3, 5] = 3
+    st[7, :4] = -2
+    seeds = np.arange(10, dtype=np.uint64) + 50
+    want_s, want_e = oracle.run(h, u, v, J, st, 1, betas, seeds, False, gibbs)
+    s, e = simulated_annealing(10, h, u, v, J, 1, betas, 0, st.copy(), False, crit, seeds=seeds)
+    np.testing.assert_array_equal(s, want_s)
+    np.testing.assert_array_equal(bits(e), bits(want_e))
+
+
 # ---- tests/test_simulated_annealing.py restated against the CUDA path -------
 
 def fm_problem(num_variables=10, num_samples=100, num_sweeps=1000):

@@ -8,7 +8,7 @@ import pytest
 import torch
 
 import oracle
-from b200sa import Plan, workloads
+from b200sa import Plan, sample_batch, workloads
 from b200sa.workloads import Instance, random_regular, random_states
 from conftest import bits
 
@@ -80,6 +80,36 @@ def test_set_weights_equals_fresh_plan():
     with Plan(probs) as plan:
         with pytest.raises(ValueError):
             plan.set_weights(len(probs), probs[0].h, probs[0].J)
+
+
+def test_set_weights_device_equals_fresh_plan():
+    """All problems' weights replaced from device tensors in one kernel,
+    including problems with in-window resolution (dense; their back-neighbour
+    couplings are copies of adjacency entries) and a captured graph."""
+    probs = mixed_batch(seed=43)[:5]
+    probs.append(workloads.dense_ising(n=60, reads=24, sweeps=30, seed=9))
+    rng = np.random.default_rng(8)
+    new = copy.deepcopy(probs)
+    for p in new:
+        p.h = rng.normal(0, 0.3, p.n)
+        p.J = rng.normal(0, 1.0, p.J.shape[0])
+    with Plan(probs) as plan, Plan(new) as fresh:
+        sin, out, en = device_buffers(plan, probs)
+        plan.run(sin, out, en, mode="graph")
+        h_cat = torch.from_numpy(np.concatenate([p.h for p in new])).cuda()
+        J_cat = torch.from_numpy(np.concatenate([p.J for p in new])).cuda()
+        stream = torch.cuda.current_stream()
+        for _ in range(2):  # the first call builds the scatter map, the second reuses it
+            plan.set_weights_device(h_cat, J_cat, stream=stream)
+            plan.run(sin, out, en, mode="graph", stream=stream)
+        _, out_f, en_f = device_buffers(fresh, new)
+        fresh.run(sin, out_f, en_f)
+        assert torch.equal(out, out_f) and torch.equal(en, en_f)
+        p = new[-1]
+        ws, we = oracle.run(p.h, p.u, p.v, p.J, p.states, p.sweeps_per_beta, p.betas, p.seeds)
+        o = int(plan.state_offsets[-2])
+        got = out[o:o + p.num_reads * p.n].cpu().numpy().reshape(p.num_reads, p.n)
+        np.testing.assert_array_equal(got, ws)
 
 
 def test_autotune_keeps_results_and_caches(tmp_path):
@@ -212,3 +242,16 @@ def test_bucket_report_matches_run_counters():
             assert sum(r["flips"] for r in rep) == st["flips"]
             assert sum(r["passes"] for r in rep) == st["passes"]
             assert all(r["ms"] > 0 and r["model_bytes"] > 0 and r["grid"] > 0 for r in rep), rep
+
+
+def test_sharded_batch_on_two_host_threads_equals_one_call():
+    """b200sa.shards on one GPU driven as two devices (two host threads, two
+    plans at once): the gathered result equals one batched call."""
+    from b200sa import shards
+    probs = mixed_batch(seed=47)
+    a, b = copy.deepcopy(probs), copy.deepcopy(probs)
+    ea = sample_batch(a, mode="persistent")
+    eb = shards.sample_batch_devices(b, devices=[0, 0])
+    for pa, pb, xa, xb in zip(a, b, ea, eb):
+        np.testing.assert_array_equal(pa.states, pb.states)
+        np.testing.assert_array_equal(bits(xa), bits(xb))

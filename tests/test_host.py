@@ -147,8 +147,15 @@ def test_ring_reproduces_stream():
     assert got == list(map(int, want))
 
 
-def _model_anneal(h, u, v, J, s, betas, spb, seed, gibbs):
-    """Speculative 32-wide windows exactly as the sequential-order kernel."""
+def _model_anneal(h, u, v, J, s, betas, spb, seed, gibbs, resolve=False):
+    """Speculative 32-wide windows exactly as the sequential-order kernel.
+
+    With ``resolve`` (used when no list names a target twice and every spin
+    is +-1), a pass does not end at the first lane a committed flip could
+    have changed: the flips just committed correct the delta energies of the
+    later lanes they neighbour (in variable order, as the reference adds
+    them), those lanes decide again with draws placed after the committed
+    ones, and the pass goes on until the window is committed."""
     n = len(h)
     rows = [[] for _ in range(n)]
     for a, b, w in zip(u, v, J):
@@ -158,6 +165,11 @@ def _model_anneal(h, u, v, J, s, betas, spb, seed, gibbs):
     for i in range(n):
         ds = [t - i for t, _ in rows[i] if t > i]
         dist.append(min([32] + ds))
+    if resolve:
+        assert all(len({t for t, _ in r}) == len(r) for r in rows)
+        assert all(int(x) in (-1, 1) for x in s)
+        # back[v]: {offset o in 1..31: J} for neighbours v - o
+        back = [{i - t: w for t, w in rows[i] if 0 < i - t < 32} for i in range(n)]
     s = [int(x) for x in s]
     de = []
     for i in range(n):
@@ -173,29 +185,40 @@ def _model_anneal(h, u, v, J, s, betas, spb, seed, gibbs):
             while p < n:
                 R.refill()
                 L = min(32, n - p)
-                need, acc = [False] * L, [False] * L
-                for k in range(L):
-                    d = de[p + k]
-                    consider = not (d >= thr)
-                    need[k] = consider if gibbs else (consider and not d <= 0.0)
-                    acc[k] = (not gibbs) and consider
-                c = 0
-                for k in range(L):
-                    if need[k]:
-                        r = float(R.get(R.q + c))
-                        c += 1
-                        d = de[p + k]
-                        if gibbs:
-                            e = math.exp(d * beta) if d * beta < 709 else math.inf
-                            acc[k] = 2.0 ** 64 > r * (1 + e)
-                        else:
-                            acc[k] = math.exp(-d * beta) * 2.0 ** 64 > r
-                commit = min([L] + [k + dist[p + k] for k in range(L) if acc[k]])
-                R.q += sum(need[:commit])
-                flips = [p + k for k in range(commit) if acc[k]]
+                d = [de[p + k] for k in range(L)]
+                c, used, flips = 0, 0, []
+                while c < L:
+                    need, acc = [False] * L, [False] * L
+                    for k in range(c, L):
+                        consider = not (d[k] >= thr)
+                        need[k] = consider if gibbs else (consider and not d[k] <= 0.0)
+                        acc[k] = (not gibbs) and consider
+                    cnt = 0
+                    for k in range(c, L):
+                        if need[k]:
+                            r = float(R.get(R.q + used + cnt))
+                            cnt += 1
+                            if gibbs:
+                                e = math.exp(d[k] * beta) if d[k] * beta < 709 else math.inf
+                                acc[k] = 2.0 ** 64 > r * (1 + e)
+                            else:
+                                acc[k] = math.exp(-d[k] * beta) * 2.0 ** 64 > r
+                    commit = min([L] + [k + dist[p + k] for k in range(c, L) if acc[k]])
+                    used += sum(need[c:commit])
+                    new = [k for k in range(c, commit) if acc[k]]
+                    flips += [p + k for k in new]
+                    c = commit
+                    if not resolve:
+                        break
+                    for k in range(c, L):  # corrections, in variable order
+                        for j in new:
+                            w = back[p + k].get(k - j)
+                            if w is not None:
+                                d[k] = d[k] + ((4.0 * s[p + j]) * w) * s[p + k]
+                R.q += used
                 if flips:
                     _model_apply_flips(rows, de, s, flips)
-                p += commit
+                p += c
     return np.array(s, np.int8)
 
 
@@ -222,6 +245,31 @@ def _model_apply_flips(rows, de, s, flips):
     for var in flips:
         s[var] = -s[var]
         de[var] = -de[var]
+
+
+@pytest.mark.parametrize("gibbs", [False, True])
+def test_in_window_resolution_model_matches_oracle(gibbs):
+    """Passes that resolve in-window dependents (dense graphs, where almost
+    every variable neighbours its successor, and a periodic lattice whose
+    rows wrap inside the window) give the reference's results."""
+    rng = np.random.default_rng(11 + gibbs)
+    cases = []
+    for n, p in ((70, 0.5), (45, 0.1)):
+        iu, ju = np.triu_indices(n, 1)
+        keep = rng.random(iu.shape[0]) < p
+        cases.append((n, iu[keep].astype(np.int32), ju[keep].astype(np.int32),
+                      rng.uniform(-1, 1, int(keep.sum())), rng.uniform(-1, 1, n)))
+    L = 5
+    lat = workloads.cubic_lattice(L=L, reads=1, sweeps=1, seed=3)
+    cases.append((L ** 3, lat.u, lat.v, lat.J, lat.h))
+    for n, u, v, J, h in cases:
+        betas = np.geomspace(0.05, 4.0, 20)
+        st = (2 * rng.integers(0, 2, (2, n)) - 1).astype(np.int8)
+        seeds = np.array([5, 0], np.uint64)
+        want, _ = oracle.run(h, u, v, J, st, 1, betas, seeds, False, gibbs)
+        for r in range(2):
+            got = _model_anneal(h, u, v, J, st[r], betas, 1, int(seeds[r]), gibbs, resolve=True)
+            np.testing.assert_array_equal(got, want[r])
 
 
 @pytest.mark.parametrize("gibbs", [False, True])
