@@ -66,7 +66,7 @@ def parse_args():
                          "one by one")
     ap.add_argument("--bm-steps", type=int, default=2,
                     help="timed Boltzmann-machine gradient steps (after one untimed step)")
-    ap.add_argument("--bm-target-reads", type=int, default=1024,
+    ap.add_argument("--bm-target-reads", type=int, default=8192,
                     help="reads behind the BM target correlations (outside the timed steps)")
     ap.add_argument("--descent-samples", type=int, default=16384,
                     help="steepest-descent leg: samples (0 skips it)")
@@ -551,11 +551,12 @@ def bench_single(args, local, world, rank, inst, label, calls, cpu_reads):
 
 def bench_bm(args, local, world):
     """Batched Boltzmann-machine learning: 64 six-regular models, n~U[256,2048],
-    ground truth J*~N(0,0.5), h*=0; per gradient step 1024 fixed-beta (beta=1)
-    Gibbs reads x 2000 sweeps of every model in one persistent batch, the
-    moments kernel backward and an Adam update (lr 1e-2).  One untimed step,
-    then `bm_steps` timed steps (host clock around each synchronized step,
-    max over ranks)."""
+    ground truth J*~N(0,0.5), h*=0, targets from 8192 reads; per gradient step
+    1024 fixed-beta (beta=1) Gibbs reads x 2000 sweeps of every model in one
+    persistent batch (autotuned launch shapes, weights written on the device),
+    the moments kernel backward and an Adam update (lr 1e-2).  One untimed
+    step (it includes the autotuner), then `bm_steps` timed steps (host clock
+    around each synchronized step, max over ranks)."""
     import torch
     from b200sa import bm
     truth = workloads.bm_models(num_models=64, n_range=(256, 2048), d=6, J_sigma=0.5, seed=5)

@@ -101,7 +101,7 @@ class ModelSampler:
     """
 
     def __init__(self, models: Sequence[IsingModel], beta: float, sweeps: int, reads: int,
-                 proposal: str = "Gibbs", device: int = 0):
+                 proposal: str = "Gibbs", device: int = 0, autotune: bool = False):
         self.models = list(models)
         self.reads = int(reads)
         self.device = int(device)
@@ -113,6 +113,9 @@ class ModelSampler:
             np.array([float(beta)]), int(sweeps), np.zeros(self.reads, np.uint64),
             proposal=proposal) for m in self.models]
         self.plan = Plan(insts, device=self.device)
+        if autotune:
+            # Launch shapes measured per size bucket (results do not depend on them).
+            self.plan.autotune(None)
         self.sin = torch.empty(max(self.plan.total_state, 1), dtype=torch.int8, device=dev)
         self.sout = torch.empty_like(self.sin)
         self.en = torch.empty(max(self.plan.total_reads, 1), dtype=torch.float64, device=dev)
@@ -267,6 +270,7 @@ class SamplingSpec:
     memory_budget: int = 1 << 30   # bytes of samples kept for backward
     recompute_chunk: int = 256     # reads per chunk when recomputing
     device: int = 0
+    autotune: bool = False         # measure launch shapes when a sampler is built
     last_samples: list = None      # set by LogPartition.forward
     last_moments: tuple = None     # set by LogPartition.backward
     samplers: dict = None          # reads per call -> ModelSampler (plan + graph reused)
@@ -278,7 +282,7 @@ class SamplingSpec:
             self.samplers = {}
         if reads not in self.samplers:
             self.samplers[reads] = ModelSampler(self.models, self.beta, self.sweeps, reads,
-                                                self.proposal, self.device)
+                                                self.proposal, self.device, self.autotune)
         return self.samplers[reads]
 
     def split(self, h_cat, J_cat):

@@ -22,7 +22,8 @@ from typing import Callable, Sequence
 import numpy as np
 import torch
 
-from .autograd import IsingModel, SamplingSpec, edge_moments, log_partition, sample_models
+from .autograd import (IsingModel, ModelSampler, SamplingSpec, edge_moments, log_partition,
+                       sample_models)
 
 
 @dataclass
@@ -39,28 +40,35 @@ class BMResult:
 
 
 def target_correlations(models: Sequence[IsingModel], hs, Js, beta: float, reads: int,
-                        sweeps: int, seed: int, device: int = 0):
+                        sweeps: int, seed: int, device: int = 0, autotune: bool = False):
     """<s_u s_v> per coupler of the ground-truth models, from `reads` fixed-beta
     Gibbs reads of `sweeps` sweeps each."""
-    samples = sample_models(models, hs, Js, beta, sweeps, reads, seed, seed + 1, 0, "Gibbs",
-                            device)
-    _, sss = edge_moments(models, samples, device)
-    return [x.to(torch.float64) / reads for x in sss]
+    sampler = ModelSampler(models, beta, sweeps, reads, "Gibbs", device, autotune)
+    try:
+        samples = sample_models(models, hs, Js, beta, sweeps, reads, seed, seed + 1, 0, "Gibbs",
+                                device, sampler)
+        _, sss = edge_moments(models, samples, device)
+        return [x.to(torch.float64) / reads for x in sss]
+    finally:
+        sampler.close()
 
 
 def fit(truth: Sequence[tuple], beta: float = 1.0, steps: int = 500, reads: int = 1024,
         sweeps: int = 2000, lr: float = 1e-2, target_reads: int = 8192,
         target_sweeps: int = 2000, seed: int = 11, device: int = 0,
-        callback: Callable[[int, float], None] | None = None) -> BMResult:
+        callback: Callable[[int, float], None] | None = None,
+        autotune: bool = True) -> BMResult:
     """Fit J (from zero, h fixed at the truth's h) to the truth's coupler
-    correlations.  `truth` is a list of (h, u, v, J) ground-truth models."""
+    correlations.  `truth` is a list of (h, u, v, J) ground-truth models.
+    With `autotune` the sampling plan's launch shapes are measured once, at
+    the first step (results are the same either way)."""
     dev = torch.device("cuda", device)
     models = [IsingModel(len(h), np.ascontiguousarray(u, np.int32), np.ascontiguousarray(v, np.int32))
               for h, u, v, _ in truth]
     hs = [np.asarray(h, np.float64) for h, _, _, _ in truth]
     t0 = time.perf_counter()
     corr_data = target_correlations(models, hs, [np.asarray(J, np.float64) for *_, J in truth],
-                                    beta, target_reads, target_sweeps, seed, device)
+                                    beta, target_reads, target_sweeps, seed, device, autotune)
     torch.cuda.synchronize(dev)
     res = BMResult(J=[], target_seconds=time.perf_counter() - t0)
     data = torch.cat(corr_data).to(dev)
@@ -72,7 +80,7 @@ def fit(truth: Sequence[tuple], beta: float = 1.0, steps: int = 500, reads: int 
         t = time.perf_counter()
         spec = SamplingSpec(models, beta=beta, sweeps=sweeps, reads=reads,
                             seed=seed + 1000 + step, init_seed=seed + 7 + step, device=device,
-                            samplers=samplers)
+                            samplers=samplers, autotune=autotune)
         loss = beta * torch.dot(J, data) + log_partition(h_cat, J, spec)
         samplers = spec.samplers
         opt.zero_grad()
@@ -91,3 +99,54 @@ def fit(truth: Sequence[tuple], beta: float = 1.0, steps: int = 500, reads: int 
         res.J.append(Jn[off:off + m.num_couplers].copy())
         off += m.num_couplers
     return res
+
+
+def main(argv=None):
+    """Run the batched fit on seeded synthetic ground truths and write the
+    correlation-error curve:
+
+        python -m b200sa.bm [--steps 500] [--models 64] [--out curve.json]
+
+    Defaults: 64 six-regular models, n ~ U[256, 2048], J* ~ N(0, 0.5), h* = 0,
+    targets from 8192 reads at beta = 1, Adam lr 1e-2, 1024 reads x 2000 Gibbs
+    sweeps per step."""
+    import argparse
+    import json
+    from . import workloads
+    ap = argparse.ArgumentParser(prog="python -m b200sa.bm")
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--models", type=int, default=64)
+    ap.add_argument("--reads", type=int, default=1024)
+    ap.add_argument("--sweeps", type=int, default=2000)
+    ap.add_argument("--target-reads", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=1e-2)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    truth = workloads.bm_models(num_models=a.models, n_range=(256, 2048), d=6, J_sigma=0.5,
+                                seed=5)
+    t0 = time.perf_counter()
+
+    def report(step, err):
+        if step % 10 == 0 or step == a.steps - 1:
+            print(f"step {step:4d}  corr_error {err:.5f}  {time.perf_counter() - t0:8.1f} s",
+                  flush=True)
+
+    res = fit(truth, beta=1.0, steps=a.steps, reads=a.reads, sweeps=a.sweeps, lr=a.lr,
+              target_reads=a.target_reads, target_sweeps=a.sweeps, seed=3, device=a.device,
+              callback=report)
+    Jerr = float(np.mean([np.mean(np.abs(J - t[3])) for J, t in zip(res.J, truth)]))
+    out = {"steps": a.steps, "models": a.models, "reads": a.reads, "sweeps": a.sweeps,
+           "target_reads": a.target_reads, "lr": a.lr, "corr_error": res.corr_error,
+           "step_seconds": res.step_seconds, "target_seconds": res.target_seconds,
+           "steps_per_second_after_first": (len(res.step_seconds) - 1) /
+                                           max(sum(res.step_seconds[1:]), 1e-9),
+           "mean_abs_J_error": Jerr}
+    if a.out:
+        with open(a.out, "w") as f:
+            json.dump(out, f)
+    print(json.dumps({k: v for k, v in out.items() if k not in ("corr_error", "step_seconds")}))
+
+
+if __name__ == "__main__":
+    main()

@@ -129,6 +129,7 @@ struct LaunchShape {
     int region;
     int grid;
     int variant;
+    int touch_bytes;   // random order: the touch bitmap inside the region
 };
 
 // Arena byte offsets of one packed problem.

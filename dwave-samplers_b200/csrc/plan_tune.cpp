@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -246,6 +247,7 @@ int time_candidate(b200sa_plan_s *P, int kind, int max_n, const TuneChoice &c, T
     a.items = S.items.ptr;
     a.num_items = S.count;
     a.smem_cap_n = s.cap_n;
+    a.touch_bytes = s.touch_bytes;
     a.scratch_de = P->scratch_de.ptr;
     a.scratch_s = P->scratch_s.ptr;
     a.scratch_stride = P->scratch_stride;
@@ -441,7 +443,8 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
             for (int regs = 0; regs < kRegClasses; ++regs)
             for (int stage : {kStageShared, kStageSpins, kStageGlobal}) {
                 if (stage == kStageShared && max_n > plan->onchip_max) continue;
-                const int region = region_bytes_for_stage(stage, stage == kStageGlobal ? 0 : max_n);
+                const int region = region_bytes_for_stage(stage, stage == kStageGlobal ? 0 : max_n) +
+                                   touch_bytes_for((kind & kKindRandom) != 0, max_n);
                 if (region > smem_blk) continue;
                 const int variant = kernel_variant(kind, stage, regs);
                 int resident[kMaxThreadsPerCta / 32 + 1] = {};
@@ -494,11 +497,23 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
                 }
             }
             float best_ms = 0.f;
+            // B200SA_TUNE_LOG names a file that receives one line per measured
+            // candidate (the evidence behind each choice).
+            const char *log_path = std::getenv("B200SA_TUNE_LOG");
+            std::ofstream tlog;
+            if (log_path && *log_path) tlog.open(log_path, std::ios::app);
             for (const TuneChoice &c : cands) {
                 float ms = 0.f;
                 rc = time_candidate(plan, kind, max_n, c, S, &ms, err, errlen);
                 if (rc) return rc;
                 ++measured;
+                if (tlog)
+                    tlog << "kind=" << kind << " max_n=" << max_n << " items=" << S.count
+                         << " staging=" << c.staging << " warps_per_cta=" << c.warps_per_cta
+                         << " ctas_per_sm=" << c.ctas_per_sm << " registers="
+                         << (c.reg_class == 1 ? kRegs80 : c.reg_class == 2 ? kRegs64 : 128)
+                         << " ms=" << ms << " attempts_per_s="
+                         << (ms > 0.f ? S.attempts / (ms * 1e-3) : 0.0) << '\n';
                 if (!best.set || ms < best_ms) {
                     best = c;
                     best_ms = ms;

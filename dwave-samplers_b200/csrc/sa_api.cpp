@@ -91,12 +91,14 @@ int occupancy(b200sa_plan_s *P, int variant, int w, int region, int *ctas, char 
 int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, bool persistent,
               LaunchShape &out, char *err, size_t errlen, const TuneChoice *choice) {
     const int smem_blk = (int)P->prop.sharedMemPerBlockOptin;
+    const int tb = touch_bytes_for((kind & kKindRandom) != 0, max_n_here);
     int stage = choice && choice->set ? choice->staging : kStageShared;
     if (stage == kStageShared && max_n_here > P->onchip_max) stage = kStageGlobal;
-    if (stage == kStageSpins && region_bytes_for_stage(kStageSpins, max_n_here) > smem_blk)
+    if (stage == kStageSpins && region_bytes_for_stage(kStageSpins, max_n_here) + tb > smem_blk)
         stage = kStageGlobal;
     const int cap = stage == kStageGlobal ? 0 : max_n_here;
-    const int region = region_bytes_for_stage(stage, cap);
+    const int region = region_bytes_for_stage(stage, cap) + tb;
+    out.touch_bytes = tb;
     const int reg_class = choice && choice->set ? choice->reg_class : 0;
     const int variant = kernel_variant(kind, stage, reg_class);
     out.stage = stage;
@@ -219,6 +221,7 @@ int launch_shape(b200sa_plan_s *P, LaunchArgs a, const LaunchShape &s, const int
     a.items = items;
     a.num_items = count;
     a.smem_cap_n = s.cap_n;
+    a.touch_bytes = s.touch_bytes;
     a.queue_head = (persistent && !shared_stream) ? qhead : nullptr;
     B200SA_CUDA(launch_sa(s.variant, a, s.grid, s.warps_per_cta, s.region, st));
     P->launches++;

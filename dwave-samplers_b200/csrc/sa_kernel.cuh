@@ -621,51 +621,122 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
     }
 }
 
-// cpu_sa.cpp:134-136: each attempt draws its variable as rand % n.  One
-// attempt per step, warp-uniform; lanes share the neighbour update.
+// Random order (cpu_sa.cpp:134-139) in speculative windows of the RNG
+// stream.  Each attempt draws its variable as rand % n and, when it needs one,
+// its acceptance draw right after it.  Lane l takes stream position q + l as
+// the variable draw of a possible attempt and q + l + 1 as that attempt's
+// acceptance draw, and decides it against the delta energies at the start of
+// the pass.  The attempts actually made form a chain: lane 0, then each
+// chain lane's successor at l + 1, or l + 2 when l drew for its acceptance.
+// A chain lane's decision stands unless an earlier accepted flip of the
+// window touched its variable (flipped it or a neighbour of it); the window
+// commits the chain up to the first such lane.  Touched variables are marked
+// in a per-warp bitmap (`touch`, n bits, clear between passes).  Committed
+// flips are pairwise distinct and non-adjacent, so their neighbour updates
+// are applied together, equal targets summed in entry order.
 template <bool GIBBS>
 __device__ __forceinline__ void sweep_random(const Prob &P, double *de,
                                              int8_t *sp, double *scratch,
                                              uint64_t *ring, RingState &rs,
-                                             unsigned lane, Counters &cnt) {
+                                             unsigned lane, Counters &cnt,
+                                             uint32_t *touch) {
     const int n = P.n;
+    const int D = P.regular_degree;
     for (int b = 0; b < P.num_betas; ++b) {
         const double beta = __ldg(&P.betas[b]);
         const double thr = __ldg(&P.thresholds[b]);
         for (int sw = 0; sw < P.sweeps_per_beta; ++sw) {
-            for (int i = 0; i < n; ++i) {
+            int rem = n;  // attempts left in this sweep
+            while (rem > 0) {
                 ring_refill(ring, rs, lane);
-                const uint64_t r1 = ring[rs.q & (kRing - 1)];
-                rs.q += 1;
-                const int var = (int)(r1 % (uint64_t)n);
+                const uint64_t rv = ring[(rs.q + lane) & (kRing - 1)];
+                const int var = (int)(rv % (uint64_t)n);  // cpu_sa.cpp:135-136
                 const double d = de[var];
-                cnt.passes += 1;
-                if (d >= thr) continue;
-                bool acc;
-                if (GIBBS) {
-                    const double rd = __ull2double_rn(ring[rs.q & (kRing - 1)]);
-                    rs.q += 1;
-                    const double y =
-                        __dmul_rn(rd, __dadd_rn(1.0, exp(__dmul_rn(d, beta))));
-                    acc = kTwo64 > y;
-                    cnt.near += fabs(y - kTwo64) <= kTwo64 * kTieRel;
-                } else if (d <= 0.0) {
-                    acc = true;
-                } else {
-                    const double rd = __ull2double_rn(ring[rs.q & (kRing - 1)]);
-                    rs.q += 1;
-                    const double x = __dmul_rn(exp(__dmul_rn(-d, beta)), kTwo64);
-                    acc = x > rd;
-                    cnt.near += fabs(x - rd) <= x * kTieRel;
+                const bool cons = !(d >= thr);            // cpu_sa.cpp:140
+                const bool need = GIBBS ? cons : (cons && !(d <= 0.0));
+                const unsigned N = __ballot_sync(kFull, need);
+                // Chain lanes: l is on the chain unless l - 1 is a chain lane
+                // that drew.  Inside a run of drawing lanes starting at a, the
+                // chain takes a, a + 2, ...; elsewhere every lane.
+                bool on = true;
+                if (lane > 0 && ((N >> (lane - 1)) & 1u)) {
+                    const unsigned starts = N & ~(N << 1);
+                    const unsigned below = starts & ((2u << (lane - 1)) - 1u);
+                    const int a = 31 - __clz(below);
+                    on = (((int)lane - a) & 1) == 0;
                 }
-                if (acc) {
-                    cnt.flips += 1;
-                    const uint2 vi = __ldg(&P.vinfo[var]);
-                    const int s_old = (int)sp[var];
+                unsigned C = __ballot_sync(kFull, on);
+                if (__popc(C) > rem) {  // the sweep ends inside the window
+                    unsigned t = C;
+                    for (int i = 0; i < rem; ++i) t &= t - 1u;
+                    C &= ~t;
+                }
+                const bool chain = (C >> lane) & 1u;
+                bool acc = false, near = false;
+                if (chain) {
+                    acc = GIBBS ? false : cons;  // Metropolis: d <= 0 accepts
+                    if (need) {
+                        const uint64_t r = ring[(rs.q + lane + 1u) & (kRing - 1)];
+                        const int x = decide<GIBBS>(d, beta, r);
+                        acc = (x & 1) != 0;
+                        near = (x & 2) != 0;
+                    }
+                }
+                const unsigned A = __ballot_sync(kFull, acc);
+                // Commit point: the first chain lane whose variable an earlier
+                // accepted flip touched.  Accepted lanes are marked in order.
+                int c = 32;
+                unsigned todo = A, marked = 0u;
+                while (todo) {
+                    const int j = __ffs(todo) - 1;
+                    if (j >= c) break;
+                    todo &= todo - 1u;
+                    marked |= 1u << j;
+                    const int vj = __shfl_sync(kFull, var, j);
+                    const uint2 vi = D ? make_uint2((uint32_t)vj * (uint32_t)D, (uint32_t)D)
+                                       : __ldg(&P.vinfo[vj]);
+                    const int deg = (int)(vi.y & kDegMask);
+                    for (int t = (int)lane; t < deg; t += 32) {
+                        const int x = __ldg(&P.col[vi.x + (uint32_t)t]);
+                        atomicOr(&touch[x >> 5], 1u << (x & 31));
+                    }
+                    if (lane == 0) atomicOr(&touch[vj >> 5], 1u << (vj & 31));
                     __syncwarp();
-                    apply_flips(P, de, sp, scratch, 1u, var, (int)vi.x,
-                                (int)(vi.y & kDegMask), s_old,
-                                (__ldg(&P.share[var]) & 1u) != 0u, lane);
+                    const bool hit = chain && (int)lane > j && ((touch[var >> 5] >> (var & 31)) & 1u);
+                    const unsigned H = __ballot_sync(kFull, hit);
+                    if (H) c = min(c, __ffs(H) - 1);
+                }
+                if (marked) {  // clear the marked words for the next pass
+                    __syncwarp();
+                    unsigned m = marked;
+                    while (m) {
+                        const int j = __ffs(m) - 1;
+                        m &= m - 1u;
+                        const int vj = __shfl_sync(kFull, var, j);
+                        const uint2 vi = D ? make_uint2((uint32_t)vj * (uint32_t)D, (uint32_t)D)
+                                           : __ldg(&P.vinfo[vj]);
+                        const int deg = (int)(vi.y & kDegMask);
+                        for (int t = (int)lane; t < deg; t += 32)
+                            touch[__ldg(&P.col[vi.x + (uint32_t)t]) >> 5] = 0u;
+                        if (lane == 0) touch[vj >> 5] = 0u;
+                    }
+                    __syncwarp();
+                }
+                const unsigned cm = C & (c >= 32 ? kFull : ((1u << c) - 1u));
+                const int last = 31 - __clz(cm);  // lane 0 is always committed
+                rs.q += (uint32_t)(last + 1) + ((N >> last) & 1u);
+                rem -= __popc(cm);
+                const unsigned fm = A & cm;
+                cnt.near += __popc(__ballot_sync(kFull, near) & cm);
+                cnt.flips += __popc(fm);
+                cnt.passes += 1;
+                if (fm) {
+                    const int s_old = (int)sp[var];
+                    const uint2 vi = D ? make_uint2((uint32_t)var * (uint32_t)D, (uint32_t)D)
+                                       : __ldg(&P.vinfo[var]);
+                    __syncwarp();
+                    apply_flips(P, de, sp, scratch, fm, var, (int)vi.x, (int)(vi.y & kDegMask),
+                                s_old, true, lane);
                 }
             }
         }
@@ -707,12 +778,12 @@ __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *
                                             double *de, int8_t *sp,
                                             double *scratch, uint64_t *ring,
                                             RingState &rs, unsigned lane,
-                                            Counters &cnt) {
+                                            Counters &cnt, uint32_t *touch) {
     const bool pm1 = load_state(PD, src, de, sp, lane);
     {
         const Prob P = load_prob(PD);
         if (RANDOM_ORDER)
-            sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt);
+            sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, touch);
         else
             sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, RESOLVE && pm1);
     }

@@ -31,7 +31,8 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
     const int64_t total_warps = (int64_t)gridDim.x * warps_per_cta;
     double *de;
     int8_t *sp;
-    uint8_t *state = region + kRing * sizeof(uint64_t) + kScratchBytes;
+    uint32_t *touch = reinterpret_cast<uint32_t *>(region + kRing * sizeof(uint64_t) + kScratchBytes);
+    uint8_t *state = region + kRing * sizeof(uint64_t) + kScratchBytes + A.touch_bytes;
     if constexpr (STAGE == kStageShared) {
         de = reinterpret_cast<double *>(state);
         sp = reinterpret_cast<int8_t *>(state + (size_t)A.smem_cap_n * sizeof(double));
@@ -43,6 +44,10 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
         sp = A.scratch_s + gw * A.scratch_stride;
     }
     if (A.shared_stream && gw != 0) return;
+    if (RANDOM_ORDER) {  // the touch bitmap starts clear; every pass clears what it sets
+        for (int i = (int)lane; i < A.touch_bytes / 4; i += 32) touch[i] = 0u;
+        __syncwarp();
+    }
 
     RingState rs;
     bool stream_live = false;
@@ -76,8 +81,8 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
         const int64_t so = PD->state_offset + (int64_t)r * PD->n;
         Counters cnt = {0ull, 0ull, 0u};
         anneal_read<GIBBS, RANDOM_ORDER, RESOLVE>(PD, A.states_in + so, A.states_out + so,
-                                            &A.energies[rd], de, sp, scratch, ring, rs, lane,
-                                            cnt);
+                                                   &A.energies[rd], de, sp, scratch, ring, rs,
+                                                   lane, cnt, touch);
         if (lane == 0) {
             A.stats[rd].flips = cnt.flips;
             A.stats[rd].passes = cnt.passes;

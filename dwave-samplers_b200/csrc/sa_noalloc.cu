@@ -372,7 +372,8 @@ extern "C" int b200sa_sample_noalloc(
     const int variant = kernel_variant(
         (proposal == B200SA_GIBBS ? kKindGibbs : 0) | (varorder == B200SA_RANDOM ? kKindRandom : 0),
         kStageShared);
-    const int region = region_bytes_for(num_vars);
+    const int tb = touch_bytes_for(varorder == B200SA_RANDOM, num_vars);
+    const int region = region_bytes_for(num_vars) + tb;
     int best_w = 1, best = 0;
     for (int wpc = 1; wpc <= kMaxThreadsPerCta / 32; ++wpc) {
         if ((size_t)wpc * (size_t)region > S.smem_optin) break;
@@ -403,6 +404,7 @@ extern "C" int b200sa_sample_noalloc(
     a.seeds = d_seeds;
     a.stats = reinterpret_cast<ReadStats *>(S.base + kOffStats);
     a.smem_cap_n = num_vars;
+    a.touch_bytes = tb;
     e = launch_sa(variant, a, grid, wpc, region, st);
     if (e == cudaSuccess) {
         noalloc_ties_kernel<<<1, 1024, 0, st>>>(S.base, num_reads, d_read_near_ties);

@@ -95,6 +95,11 @@ struct LaunchArgs {
     int8_t *scratch_s;
     int64_t scratch_stride;        // elements per slot
     int64_t num_slots;
+    // Random order: bytes of the per-warp bitmap of variables touched by the
+    // window's accepted flips (touch_bytes_for of the launch's largest n), in
+    // the shared region between the scratch and the state; 0 otherwise.
+    int32_t touch_bytes;
+    int32_t pad_;
 };
 
 // Arguments of the steepest-descent kernel (sd_kernel.cuh): one problem,
@@ -219,6 +224,11 @@ inline int region_bytes_for_stage(int stage, int cap_n) {
     if (stage == kStageShared) return region_bytes_for(cap_n);
     if (stage == kStageSpins) return kRing * 8 + kScratchBytes + ((cap_n + 15) & ~15);
     return kRing * 8 + kScratchBytes;
+}
+
+// Random order keeps a bitmap of n bits per warp (16-byte multiple).
+inline int touch_bytes_for(bool random_order, int max_n) {
+    return random_order ? (((max_n + 31) / 32) * 4 + 15) & ~15 : 0;
 }
 
 }  // namespace b200sa

@@ -13,7 +13,9 @@
 # with the working tree to machines that do not have the reference sources).
 set -euo pipefail
 
-REF="${1:-/root/reference}"
+# The reference checkout: the first argument, else $B200SA_REFERENCE_DIR,
+# else the checkout mounted beside the repository on the build machine.
+REF="${1:-${B200SA_REFERENCE_DIR:-/root/reference}}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 SA="$REF/dwave/samplers/sa"

@@ -247,6 +247,88 @@ def _model_apply_flips(rows, de, s, flips):
         de[var] = -de[var]
 
 
+def _model_anneal_random(h, u, v, J, s, betas, spb, seed, gibbs):
+    """Random order (cpu_sa.cpp:134-139) in speculative windows of the RNG
+    stream: lane l takes position q + l as the variable draw of a possible
+    attempt (var = rand % n) and position q + l + 1 as its acceptance draw.
+    The attempts actually made form a chain (the next attempt's variable draw
+    follows the previous attempt's draws); it is committed up to the first
+    attempt whose variable an earlier accepted flip of the window touched
+    (the flipped variable or a neighbour of it)."""
+    n = len(h)
+    rows = [[] for _ in range(n)]
+    for a, b, w in zip(u, v, J):
+        rows[a].append((int(b), float(w)))
+        rows[b].append((int(a), float(w)))
+    s = [int(x) for x in s]
+    de = []
+    for i in range(n):
+        f = float(h[i])
+        for t, w in rows[i]:
+            f += s[t] * w
+        de.append((-2 * s[i]) * f)
+    R = _Ring(seed)
+    for beta in betas:
+        thr = 44.36142 / beta
+        for _ in range(spb):
+            rem = n
+            while rem > 0:
+                R.refill()
+                var = [R.get(R.q + l) % n for l in range(32)]
+                d = [de[x] for x in var]
+                cons = [not (x >= thr) for x in d]
+                need = [c if gibbs else (c and not x <= 0.0) for c, x in zip(cons, d)]
+                chain, pos = [], 0
+                while pos < 32 and len(chain) < rem:
+                    chain.append(pos)
+                    pos += 1 + int(need[pos])
+                acc = {}
+                for l in chain:
+                    acc[l] = (not gibbs) and cons[l]
+                    if need[l]:
+                        r = float(R.get(R.q + l + 1))
+                        if gibbs:
+                            e = math.exp(d[l] * beta) if d[l] * beta < 709 else math.inf
+                            acc[l] = 2.0 ** 64 > r * (1 + e)
+                        else:
+                            acc[l] = math.exp(-d[l] * beta) * 2.0 ** 64 > r
+                touched, c = set(), len(chain)
+                for i, l in enumerate(chain):
+                    if var[l] in touched:
+                        c = i
+                        break
+                    if acc[l]:
+                        touched.add(var[l])
+                        touched.update(t for t, _ in rows[var[l]])
+                done = chain[:c]
+                last = done[-1]
+                R.q += last + 1 + int(need[last])
+                rem -= len(done)
+                flips = [var[l] for l in done if acc[l]]
+                if flips:
+                    _model_apply_flips(rows, de, s, flips)
+    return np.array(s, np.int8)
+
+
+@pytest.mark.parametrize("gibbs", [False, True])
+def test_random_order_window_model_matches_oracle(gibbs):
+    rng = np.random.default_rng(13 + gibbs)
+    for n, p in ((90, 0.05), (40, 0.5), (7, 0.6)):
+        iu, ju = np.triu_indices(n, 1)
+        keep = rng.random(iu.shape[0]) < p
+        u = np.concatenate([iu[keep], [2]]).astype(np.int32)   # and a self-loop
+        v = np.concatenate([ju[keep], [2]]).astype(np.int32)
+        J = rng.uniform(-1, 1, u.shape[0])
+        h = rng.uniform(-1, 1, n)
+        betas = np.geomspace(0.05, 4.0, 20)
+        st = (2 * rng.integers(0, 2, (2, n)) - 1).astype(np.int8)
+        seeds = np.array([9, 0], np.uint64)
+        want, _ = oracle.run(h, u, v, J, st, 1, betas, seeds, True, gibbs)
+        for r in range(2):
+            got = _model_anneal_random(h, u, v, J, st[r], betas, 1, int(seeds[r]), gibbs)
+            np.testing.assert_array_equal(got, want[r])
+
+
 @pytest.mark.parametrize("gibbs", [False, True])
 def test_in_window_resolution_model_matches_oracle(gibbs):
     """Passes that resolve in-window dependents (dense graphs, where almost
