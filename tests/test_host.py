@@ -372,3 +372,25 @@ def test_speculative_window_model_matches_oracle(gibbs):
         for r in range(2):
             got = _model_anneal(h, u, v, J, st[r], betas, 1, int(seeds[r]), gibbs)
             np.testing.assert_array_equal(got, want[r])
+
+
+def test_bench_cpu_sample_checks_gpu_reads():
+    """The benchmark's CPU-baseline leg compares every read it times with the
+    GPU run's output: an oracle-made output passes, a corrupted read is
+    counted as a mismatch."""
+    import bench
+    probs = workloads.uneven_batch(num_problems=3, n_range=(30, 60), reads_range=(2, 4),
+                                   sweeps_range=(5, 10), seed=19)
+    so = np.cumsum([0] + [p.num_reads * p.n for p in probs])
+    ro = np.cumsum([0] + [p.num_reads for p in probs])
+    states = np.zeros(so[-1], np.int8)
+    energies = np.zeros(ro[-1])
+    for k, p in enumerate(probs):
+        s, e = oracle.run(p.h, p.u, p.v, p.J, p.states, p.sweeps_per_beta, p.betas, p.seeds)
+        states[so[k]:so[k + 1]] = s.ravel()
+        energies[ro[k]:ro[k + 1]] = e
+    out = bench.cpu_sample(probs, 0, threads=2, max_reads=3, gpu_out=(states, energies, so, ro))
+    assert out["checked_reads"] == 3 and out["mismatches"] == 0
+    energies[ro[0]:ro[-1]] += 1.0
+    out = bench.cpu_sample(probs, 0, threads=2, max_reads=3, gpu_out=(states, energies, so, ro))
+    assert out["mismatches"] == 3
