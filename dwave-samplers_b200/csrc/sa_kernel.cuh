@@ -495,6 +495,14 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                         s_cur = (int)sp[v];
                     }
                 }
+                // The nearest back neighbour's coupling (stored last), loaded
+                // ahead: on lattices and chains it is the one the rounds need.
+                int o_near = 0;
+                double bw_near = 0.0;
+                if (resolve && bk.x) {
+                    o_near = __ffs(bk.x) - 1;
+                    bw_near = __ldg(&P.bw[bk.y + (uint32_t)__popc(bk.x) - 1u]);
+                }
                 const bool consider = act && !(d >= thr);  // cpu_sa.cpp:140
                 const bool need = GIBBS ? consider : (consider && !(d <= 0.0));
                 const unsigned nm = __ballot_sync(kFull, need);
@@ -555,7 +563,8 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                                 // Offsets are stored descending: o's rank
                                 // is the number of larger offsets.
                                 const int rank = __popcll((unsigned long long)bk.x >> (o + 1));
-                                const double wj = __ldg(&P.bw[bk.y + (uint32_t)rank]);
+                                const double wj =
+                                    o == o_near ? bw_near : __ldg(&P.bw[bk.y + (uint32_t)rank]);
                                 const double mj = ((smask >> j) & 1u) ? 4.0 : -4.0;
                                 d = __dadd_rn(d, __dmul_rn(__dmul_rn(mj, wj), sk));
                             }
