@@ -184,6 +184,7 @@ struct b200sa_plan_s {
     // graph_key (states in, states out, energies, seeds).
     std::vector<int64_t> h_items_lpt;  // host copy of items_lpt
     bool dry_run = false;  // launch_items / run_persistent: shapes and scratch only
+    bool capturing = false;  // run_persistent is being captured into the plan's graph
     cudaGraphExec_t graph_exec = nullptr;
     const void *graph_key[4] = {};
     int64_t graph_launches = 0;

@@ -39,7 +39,9 @@ int run_graph(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err, size_t
         B200SA_CUDA(cudaStreamSynchronize(P->stream));
         B200SA_CUDA(cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeRelaxed));
         P->launches = 0;
+        P->capturing = true;
         rc = run_persistent(P, a, P->stream, err, errlen);
+        P->capturing = false;
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(P->stream, &g);
         if (rc) {

@@ -93,7 +93,27 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
     const int smem_blk = (int)P->prop.sharedMemPerBlockOptin;
     const int tb = touch_bytes_for((kind & kKindRandom) != 0, max_n_here);
     int stage = choice && choice->set ? choice->staging : kStageShared;
-    if (stage == kStageShared && max_n_here > P->onchip_max) stage = kStageGlobal;
+    if (stage == kStageShared && max_n_here > P->onchip_max) {
+        stage = kStageGlobal;
+        // Untuned, above the on-chip size: keep the spins in shared memory
+        // (delta energies in the global slot) when every item still gets a
+        // resident warp that way; the spin reads of the neighbour updates
+        // then stay on chip.
+        const int spins_region = region_bytes_for_stage(kStageSpins, max_n_here) + tb;
+        if (!(choice && choice->set) && spins_region <= smem_blk) {
+            const int v2 = kernel_variant(kind, kStageSpins, 0);
+            int most = 0;
+            for (int w = 1; w <= kMaxThreadsPerCta / 32 && (int64_t)w * spins_region <= smem_blk;
+                 ++w) {
+                int ctas = 0;
+                int rc = occupancy(P, v2, w, spins_region, &ctas, err, errlen);
+                if (rc) return rc;
+                most = std::max(most, ctas * w);
+            }
+            if (most > 0 && items <= (int64_t)P->prop.multiProcessorCount * most)
+                stage = kStageSpins;
+        }
+    }
     if (stage == kStageSpins && region_bytes_for_stage(kStageSpins, max_n_here) + tb > smem_blk)
         stage = kStageGlobal;
     const int cap = stage == kStageGlobal ? 0 : max_n_here;
@@ -113,11 +133,23 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
         if (rc) return rc;
         if (ctas < 1) return set_err(err, errlen, B200SA_ECUDA, "tuned shape does not fit on an SM");
         if (choice->ctas_per_sm > 0) ctas = std::min(ctas, choice->ctas_per_sm);
+        int wl = w;
+        if (!persistent) {
+            // One problem's reads: spread them over every SM first, as the
+            // occupancy rule does (a tuned CTA width assumes a full bucket).
+            const int sms = P->prop.multiProcessorCount;
+            wl = (int)std::min<int64_t>(w, std::max<int64_t>(1, (items + sms - 1) / sms));
+            if (wl != w) {
+                int rc = occupancy(P, variant, wl, region, &ctas, err, errlen);
+                if (rc) return rc;
+                if (choice->ctas_per_sm > 0) ctas = std::min(ctas, choice->ctas_per_sm * w / wl);
+            }
+        }
         out.cap_n = cap;
-        out.warps_per_cta = w;
+        out.warps_per_cta = wl;
         out.region = region;
         out.grid = (int)std::max<int64_t>(
-            1, std::min<int64_t>((int64_t)P->prop.multiProcessorCount * ctas, (items + w - 1) / w));
+            1, std::min<int64_t>((int64_t)P->prop.multiProcessorCount * ctas, (items + wl - 1) / wl));
         out.variant = variant;
         return B200SA_OK;
     }
@@ -316,12 +348,15 @@ int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
         const int si = next++ % kStreams;
         if (!used[si]) B200SA_CUDA(cudaStreamWaitEvent(P->bstream[si], P->fork, 0));
         used[si] = true;
-        B200SA_CUDA(cudaEventRecord(P->bev[b][0], P->bstream[si]));
+        // Inside a capture the timing events become event-record nodes of the
+        // graph (external records), so every replay records them.
+        const unsigned evflags = P->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+        B200SA_CUDA(cudaEventRecordWithFlags(P->bev[b][0], P->bstream[si], evflags));
         int rc = launch_shape(P, a, shape[b], P->items_lpt.ptr + P->bucket_off[b], cnt,
                               P->bucket_max_n[b], true, false, P->qhead.ptr + b, slot0[b],
                               P->bstream[si], err, errlen);
         if (rc) return rc;
-        B200SA_CUDA(cudaEventRecord(P->bev[b][1], P->bstream[si]));
+        B200SA_CUDA(cudaEventRecordWithFlags(P->bev[b][1], P->bstream[si], evflags));
         P->bshape[b] = shape[b];
     }
     for (int si = 0; si < kStreams; ++si) {

@@ -167,6 +167,11 @@ __device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
     return q;
 }
 
+// Brings the line holding *p (global memory) into L1 without waiting.
+__device__ __forceinline__ void prefetch_l1(const void *p) {
+    asm volatile("prefetch.global.L1 [%0];" : : "l"(p));
+}
+
 __device__ __forceinline__ void xs_advance(uint64_t &s0, uint64_t &s1) {
     uint64_t a = s0;
     const uint64_t b = s1;
@@ -459,12 +464,17 @@ __device__ __forceinline__ int decide(double d, double beta, uint64_t r) {
 // with rounding, so a contribution added after the negation in the reference
 // (a neighbour that flipped earlier) equals the negated contribution added
 // before it.
+//
+// With resolution a pass commits its whole window, so the next window is
+// known while this one is processed: its records (and its delta energies when
+// they live in global memory) are prefetched into L1, and so are the lines of
+// this window's adjacency lists, which the update phase reads.
 template <bool GIBBS>
 __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                                                  int8_t *sp, double *scratch,
                                                  uint64_t *ring, RingState &rs,
                                                  unsigned lane, Counters &cnt,
-                                                 bool resolve) {
+                                                 bool resolve, bool de_global) {
     const int n = P.n;
     const int D = P.regular_degree;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -502,6 +512,19 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                 if (resolve && bk.x) {
                     o_near = __ffs(bk.x) - 1;
                     bw_near = __ldg(&P.bw[bk.y + (uint32_t)__popc(bk.x) - 1u]);
+                }
+                if (resolve && act) {
+                    const uint32_t e0 = D ? (uint32_t)v * (uint32_t)D : vi.x;
+                    prefetch_l1(P.col + e0);
+                    prefetch_l1(P.w + e0);
+                    const int vn = v + 32;  // the next window (this pass commits all of it)
+                    if (vn < n) {
+                        prefetch_l1(P.dist + vn);
+                        prefetch_l1(P.share + vn);
+                        prefetch_l1(P.back + vn);
+                        if (!D) prefetch_l1(P.vinfo + vn);
+                        if (de_global) prefetch_l1(de + vn);
+                    }
                 }
                 const bool consider = act && !(d >= thr);  // cpu_sa.cpp:140
                 const bool need = GIBBS ? consider : (consider && !(d <= 0.0));
@@ -787,14 +810,15 @@ __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *
                                             double *de, int8_t *sp,
                                             double *scratch, uint64_t *ring,
                                             RingState &rs, unsigned lane,
-                                            Counters &cnt, uint32_t *touch) {
+                                            Counters &cnt, uint32_t *touch, bool de_global) {
     const bool pm1 = load_state(PD, src, de, sp, lane);
     {
         const Prob P = load_prob(PD);
         if (RANDOM_ORDER)
             sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, touch);
         else
-            sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, RESOLVE && pm1);
+            sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, RESOLVE && pm1,
+                                    de_global);
     }
     __syncwarp();
     const double e = state_energy(PD, sp, lane);

@@ -82,7 +82,7 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
         Counters cnt = {0ull, 0ull, 0u};
         anneal_read<GIBBS, RANDOM_ORDER, RESOLVE>(PD, A.states_in + so, A.states_out + so,
                                                    &A.energies[rd], de, sp, scratch, ring, rs,
-                                                   lane, cnt, touch);
+                                                   lane, cnt, touch, STAGE != kStageShared);
         if (lane == 0) {
             A.stats[rd].flips = cnt.flips;
             A.stats[rd].passes = cnt.passes;
