@@ -465,10 +465,10 @@ __device__ __forceinline__ int decide(double d, double beta, uint64_t r) {
 // (a neighbour that flipped earlier) equals the negated contribution added
 // before it.
 //
-// With resolution a pass commits its whole window, so the next window is
-// known while this one is processed: its records (and its delta energies when
-// they live in global memory) are prefetched into L1, and so are the lines of
-// this window's adjacency lists, which the update phase reads.
+// While a window is processed, the records of the next one (and its delta
+// energies when they live in global memory) are prefetched into L1; with
+// resolution also the lines of this window's adjacency lists, which the
+// update phase reads.
 template <bool GIBBS>
 __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                                                  int8_t *sp, double *scratch,
@@ -513,17 +513,22 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                     o_near = __ffs(bk.x) - 1;
                     bw_near = __ldg(&P.bw[bk.y + (uint32_t)__popc(bk.x) - 1u]);
                 }
-                if (resolve && act) {
-                    const uint32_t e0 = D ? (uint32_t)v * (uint32_t)D : vi.x;
-                    prefetch_l1(P.col + e0);
-                    prefetch_l1(P.w + e0);
-                    const int vn = v + 32;  // the next window (this pass commits all of it)
+                if (act) {
+                    // The next window starts at p + c <= p + 32 and ends
+                    // before p + c + 32, so the lines of [v + 32] are the
+                    // ones it may need beyond this window's.
+                    const int vn = v + 32;
                     if (vn < n) {
                         prefetch_l1(P.dist + vn);
                         prefetch_l1(P.share + vn);
-                        prefetch_l1(P.back + vn);
                         if (!D) prefetch_l1(P.vinfo + vn);
                         if (de_global) prefetch_l1(de + vn);
+                        if (resolve) prefetch_l1(P.back + vn);
+                    }
+                    if (resolve) {  // the update phase's lists (no early load with resolution)
+                        const uint32_t e0 = D ? (uint32_t)v * (uint32_t)D : vi.x;
+                        prefetch_l1(P.col + e0);
+                        prefetch_l1(P.w + e0);
                     }
                 }
                 const bool consider = act && !(d >= thr);  // cpu_sa.cpp:140
