@@ -78,6 +78,9 @@ def parse_args():
                     help="dense n=100 leg (1000 geometric sweeps): reads (0 skips it)")
     ap.add_argument("--lattice-reads", type=int, default=256,
                     help="3D lattice L=32 leg (4096 linear sweeps): reads (0 skips it)")
+    ap.add_argument("--k16-reads", type=int, default=4096,
+                    help="complete graph K16 leg (fixed beta 1, 10000 Gibbs sweeps): reads "
+                         "(0 skips it)")
     return ap.parse_args()
 
 
@@ -778,6 +781,12 @@ def run_ours(args):
             args, local, world, rank, inst,
             f"3D periodic cubic lattice L=32 (32768 spins), J=+-1, h=0, {args.lattice_reads} reads "
             "x 4096 linear sweeps 0.1->3.0, Metropolis, sequential order", 1, cpu_threads())
+    if args.k16_reads > 0:
+        inst = workloads.complete_graph(reads=args.k16_reads)
+        line["k16_gibbs"] = bench_single(
+            args, local, world, rank, inst,
+            f"complete graph K16, J~N(0,0.3), h~N(0,0.1), {args.k16_reads} reads x 10000 sweeps "
+            "at fixed beta 1, Gibbs, sequential order", 3, args.k16_reads)
     if args.bm_steps > 0:
         line["bm"] = bench_bm(args, local, world)
     if args.descent_samples > 0:

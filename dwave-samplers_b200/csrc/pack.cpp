@@ -150,6 +150,19 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
         }
     }
     out.resolve = !any_dup && n > 0 && 4 * out.bw.size() >= (size_t)n;
+    out.dense = out.resolve && n <= kDenseMaxN && 16 * (size_t)m >= (size_t)n * (size_t)n;
+    out.dense_w.clear();
+    out.dense_bits.clear();
+    if (out.dense) {
+        out.dense_w.assign((size_t)n * (size_t)n, 0.0);
+        out.dense_bits.assign((size_t)n * 4, 0u);
+        for (int32_t j = 0; j < n; ++j)
+            for (int32_t e = out.row[j]; e < out.row[j + 1]; ++e) {
+                const int32_t x = out.col[e];
+                out.dense_w[(size_t)j * n + x] = out.w[e];
+                out.dense_bits[(size_t)j * 4 + (x >> 5)] |= 1u << (x & 31);
+            }
+    }
     out.regular_degree = 0;
     if (n > 0 && maxdeg > 0 && maxdeg <= 32) {
         bool reg = true;

@@ -26,6 +26,13 @@ struct PackedAdjacency {
     std::vector<double> bw;
     std::vector<int32_t> bw_src;
     bool resolve = false;         // in-window resolution enabled (ProblemDev::resolve)
+    // Dense updates (ProblemDev::dense): n <= 128, average degree >= n/8, no
+    // repeated targets.  dense_w[j*n + x] is the coupling of j and x (0 when
+    // they are not neighbours) and dense_bits[4j .. 4j+3] the 128-bit mask of
+    // j's neighbours.
+    std::vector<double> dense_w;
+    std::vector<uint32_t> dense_bits;
+    bool dense = false;
 };
 
 // Validates one problem's arguments (lengths, indices, enums, degree limit).

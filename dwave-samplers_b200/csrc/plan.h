@@ -83,8 +83,10 @@ inline void reset_stats(b200sa_stats *s) {
 // Nibble tables of the RNG jump by kHalf outputs (computed once per process).
 const uint32_t (*jump_table())[4];
 
-// Whether plans enable in-window resolution for the problems that qualify.
+// Whether plans enable in-window resolution / dense updates for the problems
+// that qualify.
 bool resolve_allowed();
+bool dense_allowed();
 
 // Buckets of the persistent mode: a size class crossed with the kernel kind
 // (acceptance rule x update order).  Each bucket's warps get a shared region
@@ -134,7 +136,7 @@ struct LaunchShape {
 
 // Arena byte offsets of one packed problem.
 struct ArenaOffsets {
-    size_t vinfo, dist, share, col, w, h, cu, cv, cw, betas, thr, back, bw;
+    size_t vinfo, dist, share, col, w, h, cu, cv, cw, betas, thr, back, bw, dw, dbits;
 };
 
 }  // namespace host

@@ -322,6 +322,18 @@ int b200sa_plan_set_weights(b200sa_plan plan, int32_t problem, const double *h, 
     if (!bw.empty())
         B200SA_CUDA(cudaMemcpyAsync(base + o.bw, bw.data(), 8 * bw.size(),
                                     cudaMemcpyHostToDevice, plan->stream));
+    // The dense coupling matrix of problems with dense updates (no repeated
+    // couplers there, so each entry is one coupler's weight).
+    std::vector<double> dw;
+    if (d.dense) {
+        dw.assign((size_t)n * (size_t)n, 0.0);
+        for (int64_t c = 0; c < m; ++c) {
+            dw[(size_t)hcu[c] * n + hcv[c]] = J[c];
+            dw[(size_t)hcv[c] * n + hcu[c]] = J[c];
+        }
+        B200SA_CUDA(cudaMemcpyAsync(base + o.dw, dw.data(), 8 * dw.size(),
+                                    cudaMemcpyHostToDevice, plan->stream));
+    }
     B200SA_CUDA(cudaStreamSynchronize(plan->stream));
     return B200SA_OK;
 }
@@ -371,6 +383,12 @@ int b200sa_plan_set_weights_device(b200sa_plan plan, const double *d_h, const do
                 src.push_back((int32_t)(joff + c));
                 dst.push_back((int64_t)(o.cw / 8) + c);
                 src.push_back((int32_t)(joff + c));
+                if (d.dense) {  // the dense coupling matrix, both triangles
+                    dst.push_back((int64_t)(o.dw / 8) + (int64_t)hcu[c] * d.n + hcv[c]);
+                    src.push_back((int32_t)(joff + c));
+                    dst.push_back((int64_t)(o.dw / 8) + (int64_t)hcv[c] * d.n + hcu[c]);
+                    src.push_back((int32_t)(joff + c));
+                }
             }
             const std::vector<int32_t> &bs = plan->bw_src[i];
             for (size_t k = 0; k < bs.size(); ++k) {

@@ -59,6 +59,16 @@ bool resolve_allowed() {
     return on;
 }
 
+// Dense updates are on unless the environment sets B200SA_DENSE=0 (results
+// are identical either way; for A/B timing).
+bool dense_allowed() {
+    static const bool on = [] {
+        const char *e = std::getenv("B200SA_DENSE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 const uint32_t (*jump_table())[4] {
     static uint32_t table[kJumpTable][4];
     static std::once_flag once;
@@ -462,6 +472,8 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         o.thr = take(8 * nb);
         o.back = take(8 * n);
         o.bw = take(8 * adj[i].bw.size());
+        o.dw = take(8 * adj[i].dense_w.size());
+        o.dbits = take(4 * adj[i].dense_bits.size());
         P->state_off[i + 1] = P->state_off[i] + (int64_t)q.num_reads * q.num_vars;
         P->read_off[i + 1] = P->read_off[i] + q.num_reads;
         P->n.push_back(q.num_vars);
@@ -493,6 +505,10 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         }
         if (!adj[i].bw.empty())
             std::memcpy(&staging[o.bw], adj[i].bw.data(), 8 * adj[i].bw.size());
+        if (!adj[i].dense_w.empty()) {
+            std::memcpy(&staging[o.dw], adj[i].dense_w.data(), 8 * adj[i].dense_w.size());
+            std::memcpy(&staging[o.dbits], adj[i].dense_bits.data(), 4 * adj[i].dense_bits.size());
+        }
         if (nb) {
             std::memcpy(&staging[o.betas], q.beta_schedule, 8 * nb);
             double *thr = reinterpret_cast<double *>(&staging[o.thr]);
@@ -539,9 +555,11 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
                                                  (uint32_t)d.regular_degree
                                            : 0u;
         d.resolve = (adj[i].resolve && resolve_allowed()) ? 1 : 0;
-        d.pad_ = 0;
+        d.dense = (d.resolve && adj[i].dense && dense_allowed()) ? 1 : 0;
         d.back = reinterpret_cast<const uint2 *>(base + o.back);
         d.bw = reinterpret_cast<const double *>(base + o.bw);
+        d.dense_w = reinterpret_cast<const double *>(base + o.dw);
+        d.dense_bits = reinterpret_cast<const uint32_t *>(base + o.dbits);
         P->bw_src[i] = std::move(adj[i].bw_src);
     }
     B200SA_CUDA(P->dprobs.alloc((size_t)std::max(num_problems, 1)));

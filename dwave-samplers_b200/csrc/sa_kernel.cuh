@@ -146,6 +146,9 @@ struct Prob {
     uint32_t regular_magic;
     const uint2 *__restrict__ back;
     const double *__restrict__ bw;
+    const double *__restrict__ dense_w;
+    const uint32_t *__restrict__ dense_bits;
+    int dense;
 };
 
 __device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
@@ -164,6 +167,9 @@ __device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
     q.regular_magic = P->regular_magic;
     q.back = P->back;
     q.bw = P->bw;
+    q.dense_w = P->dense_w;
+    q.dense_bits = P->dense_bits;
+    q.dense = P->dense;
     return q;
 }
 
@@ -432,6 +438,59 @@ __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t
     }
 }
 
+// cpu_sa.cpp:168-191 for the committed flips `fm` of the window starting at
+// p, pulled instead of pushed (problems with dense updates: n <= 128, no
+// repeated couplers).  Lane l owns the delta energies of variables l, l + 32,
+// l + 64 and l + 96; flip after flip in variable order it adds
+// ((int8)(4 s_j) J_jx) s_x to each owned slot x that neighbours j, so every
+// slot receives its additions in the reference's order.  Spins are those at
+// the start of the pass; the flipped variables' spins and own delta energies
+// change last (see sweep_sequential).  `s_cur` is each lane's window spin.
+__device__ __forceinline__ void update_dense(const Prob &P, double *de, int8_t *sp,
+                                             unsigned fm, int p, int v, int s_cur,
+                                             unsigned lane) {
+    const int n = P.n;
+    double dx[4], sx[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int x = (int)lane + 32 * i;
+        dx[i] = 0.0;
+        sx[i] = 0.0;
+        if (x < n) {
+            dx[i] = de[x];
+            sx[i] = (double)(int)sp[x];
+        }
+    }
+    unsigned touched = 0u;
+    unsigned f = fm;
+    while (f) {
+        const int j = __ffs(f) - 1;
+        f &= f - 1u;
+        const double mj = (double)(int)(int8_t)(4 * __shfl_sync(kFull, s_cur, j));
+        const int vj = p + j;
+        const uint4 bits = __ldg(reinterpret_cast<const uint4 *>(P.dense_bits) + vj);
+        const double *__restrict__ row = P.dense_w + (size_t)vj * (size_t)n;
+        const uint32_t word[4] = {bits.x, bits.y, bits.z, bits.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if ((word[i] >> lane) & 1u) {
+                const double J = __ldg(&row[(int)lane + 32 * i]);
+                dx[i] = __dadd_rn(dx[i], __dmul_rn(__dmul_rn(mj, J), sx[i]));
+                touched |= 1u << i;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        if ((touched >> i) & 1u) de[(int)lane + 32 * i] = dx[i];
+    __syncwarp();
+    if ((fm >> lane) & 1u) {  // cpu_sa.cpp:189-190, after the variable's own updates
+        sp[v] = (int8_t)(-s_cur);
+        de[v] = __dmul_rn(de[v], -1.0);
+    }
+    __syncwarp();
+}
+
 // One acceptance decision (cpu_sa.cpp:144-166) for a lane that needs a draw:
 // the single-precision bounds first, the exact double test inside the band.
 // Returns accept in bit 0 and the near-tie flag in bit 1.
@@ -469,7 +528,7 @@ __device__ __forceinline__ int decide(double d, double beta, uint64_t r) {
 // energies when they live in global memory) are prefetched into L1; with
 // resolution also the lines of this window's adjacency lists, which the
 // update phase reads.
-template <bool GIBBS>
+template <bool GIBBS, bool DENSE_OK>
 __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                                                  int8_t *sp, double *scratch,
                                                  uint64_t *ring, RingState &rs,
@@ -626,7 +685,10 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                 cnt.near += __popc(nearm);
                 cnt.flips += __popc(fm);
                 cnt.passes += 1;
-                if (fm) {
+                if (fm && DENSE_OK && P.dense) {
+                    if (!resolve) s_cur = act ? (int)sp[v] : 0;
+                    update_dense(P, de, sp, fm, p, v, s_cur, lane);
+                } else if (fm) {
                     if (!resolve) s_cur = act ? (int)sp[v] : 0;
                     // A slot can receive two additions only through a repeated
                     // target in one list or a neighbour common to two flips.
@@ -822,8 +884,8 @@ __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *
         if (RANDOM_ORDER)
             sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, touch);
         else
-            sweep_sequential<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, RESOLVE && pm1,
-                                    de_global);
+            sweep_sequential<GIBBS, RESOLVE>(P, de, sp, scratch, ring, rs, lane, cnt,
+                                             RESOLVE && pm1, de_global);
     }
     __syncwarp();
     const double e = state_energy(PD, sp, lane);

@@ -193,9 +193,11 @@ __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
         P->regular_degree = 0;  // general lists
         P->regular_magic = 0;
         P->resolve = 0;  // no back-neighbour records: passes end at the first dependent
-        P->pad_ = 0;
+        P->dense = 0;
         P->back = nullptr;
         P->bw = nullptr;
+        P->dense_w = nullptr;
+        P->dense_bits = nullptr;
     }
 }
 

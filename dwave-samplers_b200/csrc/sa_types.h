@@ -64,10 +64,17 @@ struct ProblemDev {
     // neighbours, offsets descending (the order the reference adds their
     // flips' contributions).  No list may name a target twice.
     int32_t resolve;
-    int32_t pad_;
+    // Dense updates (1: on; needs resolve): the committed flips' contributions
+    // are pulled by each variable's owner lane, flip after flip, from
+    // dense_w[j*n + x] (the coupling of j and x) where bit x of
+    // dense_bits[4j ..] is set.  n <= kDenseMaxN.
+    int32_t dense;
     const uint2 *back;
     const double *bw;
+    const double *dense_w;
+    const uint32_t *dense_bits;
 };
+constexpr int kDenseMaxN = 128;
 
 // Per-read counters written by the kernel.
 struct ReadStats {

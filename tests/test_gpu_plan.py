@@ -56,15 +56,16 @@ def test_graph_replay_equals_persistent():
 
 def test_set_weights_equals_fresh_plan():
     probs = mixed_batch(seed=37)[:6]
+    probs.append(workloads.dense_ising(n=50, reads=12, sweeps=40, seed=6))  # dense updates
     rng = np.random.default_rng(5)
     new = copy.deepcopy(probs)
-    for k in (1, 4):
+    for k in (1, 4, 6):
         new[k].h = rng.normal(0, 0.3, new[k].n)
         new[k].J = rng.normal(0, 1.0, new[k].J.shape[0])
     with Plan(probs) as plan, Plan(new) as fresh:
         sin, out, en = device_buffers(plan, probs)
         plan.run(sin, out, en, mode="graph")  # a captured graph survives the update
-        for k in (1, 4):
+        for k in (1, 4, 6):
             plan.set_weights(k, new[k].h, new[k].J)
         plan.run(sin, out, en, mode="graph")
         _, out_f, en_f = device_buffers(fresh, new)
