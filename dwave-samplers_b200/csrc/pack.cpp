@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 
 #include "sa_types.h"
@@ -150,6 +151,22 @@ void pack_adjacency(const b200sa_problem &p, PackedAdjacency &out) {
         }
     }
     out.resolve = !any_dup && n > 0 && 4 * out.bw.size() >= (size_t)n;
+    {
+        std::vector<int32_t> offs(out.col.size());
+        for (int32_t v = 0; v < n; ++v)
+            for (int32_t e = out.row[v]; e < out.row[v + 1]; ++e)
+                offs[(size_t)e] = std::abs(out.col[e] - v);
+        int32_t b = 32;
+        if (!offs.empty()) {
+            const size_t k = std::min(offs.size() - 1, (offs.size() * 97) / 100);
+            std::nth_element(offs.begin(), offs.begin() + (std::ptrdiff_t)k, offs.end());
+            b = std::max<int32_t>(32, offs[k]);
+        }
+        int64_t w = 1;
+        while (w < 2 * (int64_t)b + 128) w <<= 1;
+        out.band_b = b;
+        out.band_w = (w <= kBandMaxSlots && 2 * w <= (int64_t)n) ? (int32_t)w : 0;
+    }
     out.dense = out.resolve && n <= kDenseMaxN && 16 * (size_t)m >= (size_t)n * (size_t)n;
     out.dense_w.clear();
     out.dense_bits.clear();

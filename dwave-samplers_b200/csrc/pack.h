@@ -33,6 +33,12 @@ struct PackedAdjacency {
     std::vector<double> dense_w;
     std::vector<uint32_t> dense_bits;
     bool dense = false;
+    // Banded delta energies (ProblemDev::band_b / band_w): the smallest
+    // offset b >= 32 that covers 97% of the adjacency entries, and the ring
+    // size (power of two >= 2b + 128, at most kBandMaxSlots, at most half of
+    // n); band_w 0 when the problem is not banded.
+    int32_t band_b = 0;
+    int32_t band_w = 0;
 };
 
 // Validates one problem's arguments (lengths, indices, enums, degree limit).

@@ -87,6 +87,7 @@ const uint32_t (*jump_table())[4];
 // that qualify.
 bool resolve_allowed();
 bool dense_allowed();
+bool band_allowed();
 
 // Buckets of the persistent mode: a size class crossed with the kernel kind
 // (acceptance rule x update order).  Each bucket's warps get a shared region
@@ -132,6 +133,7 @@ struct LaunchShape {
     int grid;
     int variant;
     int touch_bytes;   // random order: the touch bitmap inside the region
+    int band_cap;      // kStageBand: slots of the delta-energy band
 };
 
 // Arena byte offsets of one packed problem.
@@ -169,6 +171,8 @@ struct b200sa_plan_s {
     std::vector<int64_t> plain_item_off;   // per problem offset into items_plain
     int64_t bucket_off[b200sa::host::kBuckets + 1] = {};  // bucket ranges in items_lpt
     int32_t bucket_max_n[b200sa::host::kBuckets] = {};
+    // Largest band ring of a bucket whose problems are all banded, else 0.
+    int32_t bucket_band_w[b200sa::host::kBuckets] = {};
     int64_t bucket_lead_cost[b200sa::host::kBuckets] = {};
     std::map<std::pair<int, int>, int> occ_cache;  // (variant*2^24 + warps, region) -> CTAs/SM
     int64_t launches = 0;  // sweep-kernel launches issued by the current run
@@ -219,14 +223,15 @@ namespace host {
 int occupancy(b200sa_plan_s *P, int variant, int w, int region, int *ctas, char *err,
               size_t errlen);
 int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, bool persistent,
-              LaunchShape &out, char *err, size_t errlen, const TuneChoice *choice = nullptr);
+              LaunchShape &out, char *err, size_t errlen, const TuneChoice *choice = nullptr,
+              int band_w_here = 0);
 int ensure_scratch(b200sa_plan_s *P, int64_t slots, int64_t stride, char *err, size_t errlen);
 LaunchArgs base_args(b200sa_plan_s *P, const int8_t *in, int8_t *out, double *en,
                      const uint64_t *seeds);
 int launch_items(b200sa_plan_s *P, LaunchArgs a, int kind, const int64_t *items, int64_t count,
                  int32_t max_n_here, bool persistent, bool shared_stream,
                  unsigned long long *qhead, cudaStream_t st, char *err, size_t errlen,
-                 const TuneChoice *choice = nullptr);
+                 const TuneChoice *choice = nullptr, int band_w_here = 0);
 int collect_stats(b200sa_plan_s *P, const std::vector<std::pair<int, int>> &ranges,
                   b200sa_stats *stats, char *err, size_t errlen);
 int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err, size_t errlen);

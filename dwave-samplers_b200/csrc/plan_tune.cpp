@@ -95,7 +95,7 @@ std::map<std::string, TuneChoice> load_cache(const char *path) {
         double rate = 0.0;
         if (!(in >> key >> staging >> w >> ctas >> regs >> rate)) continue;
         if (w < 1 || w > kMaxThreadsPerCta / 32 || ctas < 0 || regs < 0 || regs >= kRegClasses ||
-            staging < kStageGlobal || staging > kStageSpins)
+            staging < kStageGlobal || staging > kStageBand)
             continue;
         TuneChoice c;
         c.set = true;
@@ -230,10 +230,10 @@ int build_sample(b200sa_plan_s *P, int b, int64_t max_items, TuneSample &S, int 
 }
 
 // Best of two timed launches of one candidate on the sample (ms).
-int time_candidate(b200sa_plan_s *P, int kind, int max_n, const TuneChoice &c, TuneSample &S,
-                   float *best_ms, char *err, size_t errlen) {
+int time_candidate(b200sa_plan_s *P, int kind, int max_n, int band_w, const TuneChoice &c,
+                   TuneSample &S, float *best_ms, char *err, size_t errlen) {
     LaunchShape s{};
-    int rc = shape_for(P, kind, max_n, S.count, true, s, err, errlen, &c);
+    int rc = shape_for(P, kind, max_n, S.count, true, s, err, errlen, &c, band_w);
     if (rc) return rc;
     if (s.stage != kStageShared) {
         rc = ensure_scratch(P, (int64_t)s.grid * s.warps_per_cta, max_n, err, errlen);
@@ -250,6 +250,7 @@ int time_candidate(b200sa_plan_s *P, int kind, int max_n, const TuneChoice &c, T
     a.num_items = S.count;
     a.smem_cap_n = s.cap_n;
     a.touch_bytes = s.touch_bytes;
+    a.band_cap = s.band_cap;
     a.scratch_de = P->scratch_de.ptr;
     a.scratch_s = P->scratch_s.ptr;
     a.scratch_stride = P->scratch_stride;
@@ -441,6 +442,7 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
         if (cnt <= 0) continue;
         const int kind = b % kKinds;
         const int max_n = plan->bucket_max_n[b];
+        const int band_w = plan->bucket_band_w[b];
         TuneSample S;
         int mean_degree = 0;
         int rc = build_sample(plan, b, (int64_t)sms * kTuneWarpsPerSm, S, &mean_degree,
@@ -461,10 +463,13 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
             // with one CTA fewer per SM (more L1 beside the shared regions).
             std::vector<TuneChoice> cands;
             for (int regs = 0; regs < kRegClasses; ++regs)
-            for (int stage : {kStageShared, kStageSpins, kStageGlobal}) {
+            for (int stage : {kStageShared, kStageSpins, kStageGlobal, kStageBand}) {
                 if (stage == kStageShared && max_n > plan->onchip_max) continue;
-                const int region = region_bytes_for_stage(stage, stage == kStageGlobal ? 0 : max_n) +
-                                   touch_bytes_for((kind & kKindRandom) != 0, max_n);
+                if (stage == kStageBand && (!band_w || (kind & kKindRandom))) continue;
+                const int region =
+                    region_bytes_for_stage(stage, stage == kStageGlobal ? 0 : max_n,
+                                           stage == kStageBand ? band_w : 0) +
+                    touch_bytes_for((kind & kKindRandom) != 0, max_n);
                 if (region > smem_blk) continue;
                 const int variant = kernel_variant(kind, stage, regs);
                 int resident[kMaxThreadsPerCta / 32 + 1] = {};
@@ -498,7 +503,7 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
                 // variable, and spins for the global location).  Offer the
                 // widest CTA with its CTAs per SM capped so that the slots
                 // fit in 40% and in 70% of L2.
-                if (widest && stage != kStageShared) {
+                if (widest && (stage == kStageGlobal || stage == kStageSpins)) {
                     const double per_warp = (double)max_n * (stage == kStageGlobal ? 9.0 : 8.0);
                     const double l2 = (double)plan->prop.l2CacheSize;
                     int last_cap = ctas_of[widest] - 1;
@@ -524,7 +529,7 @@ int b200sa_plan_autotune(b200sa_plan plan, const char *cache_path, int32_t flags
             if (log_path && *log_path) tlog.open(log_path, std::ios::app);
             for (const TuneChoice &c : cands) {
                 float ms = 0.f;
-                rc = time_candidate(plan, kind, max_n, c, S, &ms, err, errlen);
+                rc = time_candidate(plan, kind, max_n, band_w, c, S, &ms, err, errlen);
                 if (rc) return rc;
                 ++measured;
                 if (tlog)

@@ -59,6 +59,16 @@ bool resolve_allowed() {
     return on;
 }
 
+// Banded delta energies are on unless the environment sets B200SA_BAND=0
+// (results are identical either way; for A/B timing).
+bool band_allowed() {
+    static const bool on = [] {
+        const char *e = std::getenv("B200SA_BAND");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 // Dense updates are on unless the environment sets B200SA_DENSE=0 (results
 // are identical either way; for A/B timing).
 bool dense_allowed() {
@@ -99,27 +109,50 @@ int occupancy(b200sa_plan_s *P, int variant, int w, int region, int *ctas, char 
 // slot, L2-resident).  Untuned, state is in shared memory whenever it fits
 // and warps per CTA maximize resident warps per SM.
 int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, bool persistent,
-              LaunchShape &out, char *err, size_t errlen, const TuneChoice *choice) {
+              LaunchShape &out, char *err, size_t errlen, const TuneChoice *choice,
+              int band_w_here) {
     const int smem_blk = (int)P->prop.sharedMemPerBlockOptin;
     const int tb = touch_bytes_for((kind & kKindRandom) != 0, max_n_here);
+    if (kind & kKindRandom) band_w_here = 0;  // the band follows a sequential window
     int stage = choice && choice->set ? choice->staging : kStageShared;
+    if (stage == kStageBand &&
+        (!band_w_here ||
+         region_bytes_for_stage(kStageBand, max_n_here, band_w_here) + tb > smem_blk))
+        stage = kStageSpins;
+    // The most resident warps per SM a location allows (occupancy rule).
+    auto most_warps = [&](int st, int region, int *most) {
+        *most = 0;
+        const int var = kernel_variant(kind, st, 0);
+        for (int w = 1; w <= kMaxThreadsPerCta / 32 && (int64_t)w * region <= smem_blk; ++w) {
+            int ctas = 0;
+            int rc = occupancy(P, var, w, region, &ctas, err, errlen);
+            if (rc) return rc;
+            *most = std::max(*most, ctas * w);
+        }
+        return (int)B200SA_OK;
+    };
     if (stage == kStageShared && max_n_here > P->onchip_max) {
         stage = kStageGlobal;
+        // Untuned, above the on-chip size, banded: the band location (spins
+        // and the band of delta energies around the window on chip) when
+        // every item still gets a resident warp that way.
+        const int band_region = region_bytes_for_stage(kStageBand, max_n_here, band_w_here) + tb;
+        if (!(choice && choice->set) && band_w_here && band_region <= smem_blk) {
+            int most = 0;
+            int rc = most_warps(kStageBand, band_region, &most);
+            if (rc) return rc;
+            if (most > 0 && items <= (int64_t)P->prop.multiProcessorCount * most)
+                stage = kStageBand;
+        }
         // Untuned, above the on-chip size: keep the spins in shared memory
         // (delta energies in the global slot) when every item still gets a
         // resident warp that way; the spin reads of the neighbour updates
         // then stay on chip.
         const int spins_region = region_bytes_for_stage(kStageSpins, max_n_here) + tb;
-        if (!(choice && choice->set) && spins_region <= smem_blk) {
-            const int v2 = kernel_variant(kind, kStageSpins, 0);
+        if (stage == kStageGlobal && !(choice && choice->set) && spins_region <= smem_blk) {
             int most = 0;
-            for (int w = 1; w <= kMaxThreadsPerCta / 32 && (int64_t)w * spins_region <= smem_blk;
-                 ++w) {
-                int ctas = 0;
-                int rc = occupancy(P, v2, w, spins_region, &ctas, err, errlen);
-                if (rc) return rc;
-                most = std::max(most, ctas * w);
-            }
+            int rc = most_warps(kStageSpins, spins_region, &most);
+            if (rc) return rc;
             if (most > 0 && items <= (int64_t)P->prop.multiProcessorCount * most)
                 stage = kStageSpins;
         }
@@ -127,8 +160,10 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
     if (stage == kStageSpins && region_bytes_for_stage(kStageSpins, max_n_here) + tb > smem_blk)
         stage = kStageGlobal;
     const int cap = stage == kStageGlobal ? 0 : max_n_here;
-    const int region = region_bytes_for_stage(stage, cap) + tb;
+    const int band_cap = stage == kStageBand ? band_w_here : 0;
+    const int region = region_bytes_for_stage(stage, cap, band_cap) + tb;
     out.touch_bytes = tb;
+    out.band_cap = band_cap;
     const int reg_class = choice && choice->set ? choice->reg_class : 0;
     const int variant = kernel_variant(kind, stage, reg_class);
     out.stage = stage;
@@ -234,10 +269,10 @@ LaunchArgs base_args(b200sa_plan_s *P, const int8_t *in, int8_t *out, double *en
 // work-queue head `qhead` (zeroed by the caller, stream-ordered).
 int items_shape(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t count, bool persistent,
                 bool shared_stream, const TuneChoice *choice, LaunchShape &s, char *err,
-                size_t errlen) {
+                size_t errlen, int band_w_here = 0) {
     int rc = shape_for(P, kind, max_n_here, shared_stream ? 1 : count,
                        persistent && !shared_stream, s, err, errlen,
-                       shared_stream ? nullptr : choice);
+                       shared_stream ? nullptr : choice, band_w_here);
     if (rc) return rc;
     if (shared_stream) {  // one stream continued read after read: one warp
         s.grid = 1;
@@ -264,6 +299,7 @@ int launch_shape(b200sa_plan_s *P, LaunchArgs a, const LaunchShape &s, const int
     a.num_items = count;
     a.smem_cap_n = s.cap_n;
     a.touch_bytes = s.touch_bytes;
+    a.band_cap = s.band_cap;
     a.queue_head = (persistent && !shared_stream) ? qhead : nullptr;
     B200SA_CUDA(launch_sa(s.variant, a, s.grid, s.warps_per_cta, s.region, st));
     P->launches++;
@@ -273,11 +309,11 @@ int launch_shape(b200sa_plan_s *P, LaunchArgs a, const LaunchShape &s, const int
 int launch_items(b200sa_plan_s *P, LaunchArgs a, int kind, const int64_t *items,
                  int64_t count, int32_t max_n_here, bool persistent, bool shared_stream,
                  unsigned long long *qhead, cudaStream_t st, char *err, size_t errlen,
-                 const TuneChoice *choice) {
+                 const TuneChoice *choice, int band_w_here) {
     if (count <= 0) return B200SA_OK;
     LaunchShape s{};
     int rc = items_shape(P, kind, max_n_here, count, persistent, shared_stream, choice, s, err,
-                         errlen);
+                         errlen, band_w_here);
     if (rc) return rc;
     if (s.stage != kStageShared) {
         rc = ensure_scratch(P, (int64_t)s.grid * s.warps_per_cta, max_n_here, err, errlen);
@@ -328,7 +364,7 @@ int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
         const int64_t cnt = P->bucket_off[b + 1] - P->bucket_off[b];
         if (cnt <= 0) continue;
         int rc = items_shape(P, b % kKinds, P->bucket_max_n[b], cnt, true, false, &P->tune[b],
-                             shape[b], err, errlen);
+                             shape[b], err, errlen, P->bucket_band_w[b]);
         if (rc) return rc;
         if (shape[b].stage != kStageShared) {
             slot0[b] = slots;
@@ -560,6 +596,8 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         d.bw = reinterpret_cast<const double *>(base + o.bw);
         d.dense_w = reinterpret_cast<const double *>(base + o.dw);
         d.dense_bits = reinterpret_cast<const uint32_t *>(base + o.dbits);
+        d.band_b = adj[i].band_b;
+        d.band_w = band_allowed() ? adj[i].band_w : 0;
         P->bw_src[i] = std::move(adj[i].bw_src);
     }
     B200SA_CUDA(P->dprobs.alloc((size_t)std::max(num_problems, 1)));
@@ -607,6 +645,20 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
         P->bucket_lead_cost[b] = std::max(P->bucket_lead_cost[b], cost(it));
     }
     for (int b = 0; b < kBuckets; ++b) P->bucket_off[b + 1] += P->bucket_off[b];
+    // A bucket may use the band location when all of its problems are banded.
+    {
+        bool all[kBuckets];
+        for (int b = 0; b < kBuckets; ++b) all[b] = true;
+        for (int64_t it : lpt) {
+            const int p = (int)(it >> 32);
+            const int b = bucket_of(it);
+            const int32_t w = P->hprobs[p].band_w;
+            if (w == 0) all[b] = false;
+            P->bucket_band_w[b] = std::max(P->bucket_band_w[b], w);
+        }
+        for (int b = 0; b < kBuckets; ++b)
+            if (!all[b]) P->bucket_band_w[b] = 0;
+    }
 
     B200SA_CUDA(P->dseeds.alloc(std::max<size_t>(seeds.size(), 1)));
     B200SA_CUDA(P->dstats.alloc(std::max<size_t>(seeds.size(), 1)));
@@ -687,7 +739,7 @@ int b200sa_plan_run(b200sa_plan plan, int32_t mode, const int8_t *d_states_in,
                       : nullptr;
             rc = launch_items(plan, a, kind, plan->items_plain.ptr + o,
                               plan->plain_item_off[i + 1] - o, plan->n[i], false, false,
-                              nullptr, st, err, errlen, choice);
+                              nullptr, st, err, errlen, choice, plan->hprobs[i].band_w);
         }
     }
     if (rc) return rc;
@@ -845,7 +897,7 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
         } else {
             LaunchShape s{};
             rc = shape_for(plan, kind_of(plan->hprobs[0]), num_vars, num_reads, true, s, err,
-                           errlen);
+                           errlen, nullptr, plan->hprobs[0].band_w);
             if (rc) return rc;
             int ctas = 0;
             rc = occupancy(plan, s.variant, s.warps_per_cta, s.region, &ctas, err, errlen);
@@ -867,7 +919,8 @@ int b200sa_sample(int32_t num_vars, const double *h, int64_t num_couplers,
                                     plan->stream));
         B200SA_CUDA(cudaEventRecord(plan->ev0, plan->stream));
         rc = launch_items(plan, a, kind_of(plan->hprobs[0]), plan->items_plain.ptr + done, cnt,
-                          num_vars, !shared, shared, plan->qhead.ptr, plan->stream, err, errlen);
+                          num_vars, !shared, shared, plan->qhead.ptr, plan->stream, err, errlen,
+                          nullptr, plan->hprobs[0].band_w);
         if (rc) return rc;
         B200SA_CUDA(cudaEventRecord(plan->ev1, plan->stream));
         B200SA_CUDA(cudaStreamSynchronize(plan->stream));

@@ -178,6 +178,34 @@ __device__ __forceinline__ void prefetch_l1(const void *p) {
     asm volatile("prefetch.global.L1 [%0];" : : "l"(p));
 }
 
+// Delta energies of a banded problem (kStageBand): the slots of the
+// variables in [lo, lo + w) live in a shared-memory ring (`b`, w a power of
+// two, slot x & (w - 1)); every other variable's slot is in the global array
+// `g`.  The band slides with the window (see sweep_sequential).  With w = 0
+// everything is global.
+struct BandDe {
+    double *g;
+    double *b;
+    int lo;
+    unsigned w;
+    __device__ __forceinline__ double &operator[](int x) const {
+        return (unsigned)(x - lo) < w ? b[(unsigned)x & (w - 1u)] : g[x];
+    }
+};
+
+// 8-byte asynchronous copy global -> shared (completes at cp_async_wait).
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" : : "r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" : : : "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" : : "n"(N) : "memory");
+}
+
 __device__ __forceinline__ void xs_advance(uint64_t &s0, uint64_t &s1) {
     uint64_t a = s0;
     const uint64_t b = s1;
@@ -299,7 +327,8 @@ __device__ __forceinline__ bool load_state(const ProblemDev *PD, const int8_t *s
 // non-adjacent.  Entries are applied lane-parallel in rounds of 32; equal
 // targets within a round are summed in entry order by their first lane.
 // `scratch` holds 32 doubles followed by 32 ints.
-__device__ __forceinline__ void apply_flips(const Prob &P, double *de, int8_t *sp,
+template <class DE>
+__device__ __forceinline__ void apply_flips(const Prob &P, DE de, int8_t *sp,
                                             double *scratch, unsigned fm, int v,
                                             int start, int deg, int s_old,
                                             bool may_conflict, unsigned lane) {
@@ -384,7 +413,8 @@ __device__ __forceinline__ void apply_flips(const Prob &P, double *de, int8_t *s
 // prefix of the accepted ones); the other entries are loaded here.  Equal
 // targets within a round are summed in entry order by their first lane, as in
 // apply_flips.
-__device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t *sp,
+template <class DE>
+__device__ __forceinline__ void update_regular(const Prob &P, DE de, int8_t *sp,
                                                double *scratch, const int *rank_tab,
                                                int nflips, int p, bool pre, int nb0, double w0,
                                                int k0, int nb1, double w1, int k1,
@@ -446,7 +476,8 @@ __device__ __forceinline__ void update_regular(const Prob &P, double *de, int8_t
 // slot receives its additions in the reference's order.  Spins are those at
 // the start of the pass; the flipped variables' spins and own delta energies
 // change last (see sweep_sequential).  `s_cur` is each lane's window spin.
-__device__ __forceinline__ void update_dense(const Prob &P, double *de, int8_t *sp,
+template <class DE>
+__device__ __forceinline__ void update_dense(const Prob &P, DE de, int8_t *sp,
                                              unsigned fm, int p, int v, int s_cur,
                                              unsigned lane) {
     const int n = P.n;
@@ -528,22 +559,71 @@ __device__ __forceinline__ int decide(double d, double beta, uint64_t r) {
 // energies when they live in global memory) are prefetched into L1; with
 // resolution also the lines of this window's adjacency lists, which the
 // update phase reads.
-template <bool GIBBS, bool DENSE_OK>
-__device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
+//
+// BANDED (kStageBand): the delta energies of variables within band_b of the
+// window live in a shared-memory ring of band_w slots (BandDe), the rest in
+// the global slot `de_g`.  After each pass the band slides by the committed
+// count: the slots leaving it are written back and the ones entering are
+// fetched asynchronously; band_w >= 2 band_b + 128 keeps every fetch at least
+// two passes ahead of its first use (cp.async.wait_group 1 at each pass).  At
+// every sweep the band is written back and reloaded from the start.
+template <bool BANDED>
+struct DeSel {
+    using T = double *;
+};
+template <>
+struct DeSel<true> {
+    using T = BandDe;
+};
+
+template <bool GIBBS, bool DENSE_OK, bool BANDED>
+__device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                                                  int8_t *sp, double *scratch,
                                                  uint64_t *ring, RingState &rs,
                                                  unsigned lane, Counters &cnt,
-                                                 bool resolve, bool de_global) {
+                                                 bool resolve, bool de_global, double *band,
+                                                 int band_w, int band_b) {
     const int n = P.n;
     const int D = P.regular_degree;
     const unsigned lt_mask = (1u << lane) - 1u;
     int *rank_tab = reinterpret_cast<int *>(scratch + 32);
+    typename DeSel<BANDED>::T de;
+    bool band_live = false;
+    if constexpr (BANDED)
+        de = BandDe{de_g, band, 0, (unsigned)band_w};
+    else
+        de = de_g;
     for (int b = 0; b < P.num_betas; ++b) {
         const double beta = __ldg(&P.betas[b]);
         const double thr = __ldg(&P.thresholds[b]);
         for (int sw = 0; sw < P.sweeps_per_beta; ++sw) {
+            if constexpr (BANDED) {
+                if (band_w) {  // write the band back, reload it at the start
+                    cp_async_wait<0>();
+                    __syncwarp();
+                    const unsigned mask = (unsigned)band_w - 1u;
+                    if (band_live) {
+                        for (int i = (int)lane; i < band_w; i += 32) {
+                            const int x = de.lo + i;
+                            if (x >= 0 && x < n) de_g[x] = band[(unsigned)x & mask];
+                        }
+                        __syncwarp();
+                    }
+                    de.lo = -band_b;
+                    const int top = min(n, band_w - band_b);
+                    for (int x = (int)lane; x < top; x += 32) band[(unsigned)x & mask] = de_g[x];
+                    __syncwarp();
+                    band_live = true;
+                }
+            }
             int p = 0;
             while (p < n) {
+                if constexpr (BANDED) {
+                    if (band_w) {  // the slides of all but the last pass have landed
+                        cp_async_wait<1>();
+                        __syncwarp();
+                    }
+                }
                 ring_refill(ring, rs, lane);
                 const int L = min(32, n - p);
                 const int v = p + (int)lane;
@@ -581,7 +661,7 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                         prefetch_l1(P.dist + vn);
                         prefetch_l1(P.share + vn);
                         if (!D) prefetch_l1(P.vinfo + vn);
-                        if (de_global) prefetch_l1(de + vn);
+                        if (!BANDED && de_global) prefetch_l1(de_g + vn);
                         if (resolve) prefetch_l1(P.back + vn);
                     }
                     if (resolve) {  // the update phase's lists (no early load with resolution)
@@ -714,8 +794,29 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de,
                                     (int)(vi.y & kDegMask), s_cur, may_conflict, lane);
                     }
                 }
+                if constexpr (BANDED) {
+                    if (band_w) {  // slide the band by c
+                        __syncwarp();
+                        if ((int)lane < c) {
+                            const int xo = p - band_b + (int)lane;  // < p: band_b >= 32
+                            const unsigned slot = (unsigned)xo & ((unsigned)band_w - 1u);
+                            if (xo >= 0) de_g[xo] = band[slot];
+                            const int xn = xo + band_w;
+                            if (xn < n) cp_async8(&band[slot], &de_g[xn]);
+                        }
+                        cp_async_commit();
+                        __syncwarp();
+                    }
+                }
                 p += c;
+                if constexpr (BANDED) de.lo = p - band_b;
             }
+        }
+    }
+    if constexpr (BANDED) {
+        if (band_w) {  // nothing of this read may land after it
+            cp_async_wait<0>();
+            __syncwarp();
         }
     }
 }
@@ -871,21 +972,27 @@ __device__ __forceinline__ double state_energy(const ProblemDev *PD, const int8_
     return e;
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE>
+template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE, bool BANDED>
 __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *src,
                                             int8_t *dst, double *energy_out,
                                             double *de, int8_t *sp,
                                             double *scratch, uint64_t *ring,
                                             RingState &rs, unsigned lane,
-                                            Counters &cnt, uint32_t *touch, bool de_global) {
+                                            Counters &cnt, uint32_t *touch, bool de_global,
+                                            double *band, int band_cap) {
     const bool pm1 = load_state(PD, src, de, sp, lane);
     {
         const Prob P = load_prob(PD);
-        if (RANDOM_ORDER)
+        if constexpr (RANDOM_ORDER) {
             sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, touch);
-        else
-            sweep_sequential<GIBBS, RESOLVE>(P, de, sp, scratch, ring, rs, lane, cnt,
-                                             RESOLVE && pm1, de_global);
+        } else {
+            // A problem whose band does not fit the launch's ring keeps all of
+            // its delta energies in the global slot.
+            const int bw = (BANDED && PD->band_w > 0 && PD->band_w <= band_cap) ? PD->band_w : 0;
+            sweep_sequential<GIBBS, RESOLVE, BANDED>(P, de, sp, scratch, ring, rs, lane, cnt,
+                                                     RESOLVE && pm1, de_global, band, bw,
+                                                     PD->band_b);
+        }
     }
     __syncwarp();
     const double e = state_energy(PD, sp, lane);

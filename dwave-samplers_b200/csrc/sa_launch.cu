@@ -33,12 +33,15 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
     int8_t *sp;
     uint32_t *touch = reinterpret_cast<uint32_t *>(region + kRing * sizeof(uint64_t) + kScratchBytes);
     uint8_t *state = region + kRing * sizeof(uint64_t) + kScratchBytes + A.touch_bytes;
+    double *band = nullptr;
     if constexpr (STAGE == kStageShared) {
         de = reinterpret_cast<double *>(state);
         sp = reinterpret_cast<int8_t *>(state + (size_t)A.smem_cap_n * sizeof(double));
-    } else if constexpr (STAGE == kStageSpins) {
+    } else if constexpr (STAGE == kStageSpins || STAGE == kStageBand) {
         de = A.scratch_de + gw * A.scratch_stride;
         sp = reinterpret_cast<int8_t *>(state);
+        if constexpr (STAGE == kStageBand)
+            band = reinterpret_cast<double *>(state + (((size_t)A.smem_cap_n + 15) & ~size_t(15)));
     } else {
         de = A.scratch_de + gw * A.scratch_stride;
         sp = A.scratch_s + gw * A.scratch_stride;
@@ -80,9 +83,9 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
         }
         const int64_t so = PD->state_offset + (int64_t)r * PD->n;
         Counters cnt = {0ull, 0ull, 0u};
-        anneal_read<GIBBS, RANDOM_ORDER, RESOLVE>(PD, A.states_in + so, A.states_out + so,
-                                                   &A.energies[rd], de, sp, scratch, ring, rs,
-                                                   lane, cnt, touch, STAGE != kStageShared);
+        anneal_read<GIBBS, RANDOM_ORDER, RESOLVE, STAGE == kStageBand>(
+            PD, A.states_in + so, A.states_out + so, &A.energies[rd], de, sp, scratch, ring, rs,
+            lane, cnt, touch, STAGE != kStageShared, band, A.band_cap);
         if (lane == 0) {
             A.stats[rd].flips = cnt.flips;
             A.stats[rd].passes = cnt.passes;
@@ -129,12 +132,16 @@ using KernelFn = void (*)(LaunchArgs, int, int);
     name<false, false, false, stage>, name<true, false, false, stage>,                 \
         name<false, true, false, stage>, name<true, true, false, stage>,               \
         name<false, false, true, stage>, name<true, false, true, stage>, nullptr, nullptr
+// The band location exists for sequential order only.
+#define B200SA_SEQ_KINDS(name, stage)                                                  \
+    name<false, false, false, stage>, name<true, false, false, stage>, nullptr, nullptr, \
+        name<false, false, true, stage>, name<true, false, true, stage>, nullptr, nullptr
 #define B200SA_KERNEL_TABLE(name)                                                      \
     {B200SA_KINDS(name, kStageGlobal), B200SA_KINDS(name, kStageShared),              \
-     B200SA_KINDS(name, kStageSpins)}
+     B200SA_KINDS(name, kStageSpins), B200SA_SEQ_KINDS(name, kStageBand)}
 
 static KernelFn kernel_for(int variant) {
-    constexpr int kPerClass = 3 * kNumKinds;
+    constexpr int kPerClass = kNumStages * kNumKinds;
     static const KernelFn k128[kPerClass] = B200SA_KERNEL_TABLE(sa_warp_kernel);
     static const KernelFn k80[kPerClass] = B200SA_KERNEL_TABLE(sa_warp_kernel_r80);
     static const KernelFn k64[kPerClass] = B200SA_KERNEL_TABLE(sa_warp_kernel_r64);

@@ -198,6 +198,8 @@ __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
         P->bw = nullptr;
         P->dense_w = nullptr;
         P->dense_bits = nullptr;
+        P->band_b = 0;
+        P->band_w = 0;
     }
 }
 

@@ -73,8 +73,14 @@ struct ProblemDev {
     const double *bw;
     const double *dense_w;
     const uint32_t *dense_bits;
+    // Banded delta energies (kStageBand): adjacency entries mostly within
+    // band_b of their variable; band_w is the shared-memory ring size (a power
+    // of two >= 2 band_b + 128), 0 when the problem is not banded.
+    int32_t band_b;
+    int32_t band_w;
 };
 constexpr int kDenseMaxN = 128;
+constexpr int kBandMaxSlots = 8192;  // 64 KB of delta energies per warp at most
 
 // Per-read counters written by the kernel.
 struct ReadStats {
@@ -106,7 +112,8 @@ struct LaunchArgs {
     // window's accepted flips (touch_bytes_for of the launch's largest n), in
     // the shared region between the scratch and the state; 0 otherwise.
     int32_t touch_bytes;
-    int32_t pad_;
+    // kStageBand: slots of the per-warp delta-energy band (0 otherwise).
+    int32_t band_cap;
 };
 
 // Arguments of the steepest-descent kernel (sd_kernel.cuh): one problem,
@@ -227,9 +234,15 @@ inline int region_bytes_for(int cap_n) {
 constexpr int kStageGlobal = 0;
 constexpr int kStageShared = 1;
 constexpr int kStageSpins = 2;
-inline int region_bytes_for_stage(int stage, int cap_n) {
+// kStageBand: spins in the shared region, the delta energies of a band of
+// variables around the window in a shared-memory ring after them (band_cap
+// slots), the others in the global slot (sequential order, banded problems).
+constexpr int kStageBand = 3;
+constexpr int kNumStages = 4;
+inline int region_bytes_for_stage(int stage, int cap_n, int band_cap = 0) {
     if (stage == kStageShared) return region_bytes_for(cap_n);
     if (stage == kStageSpins) return kRing * 8 + kScratchBytes + ((cap_n + 15) & ~15);
+    if (stage == kStageBand) return kRing * 8 + kScratchBytes + ((cap_n + 15) & ~15) + 8 * band_cap;
     return kRing * 8 + kScratchBytes;
 }
 

@@ -208,7 +208,9 @@ typedef struct {
     int32_t max_n;
     int64_t items;          /* reads in the bucket */
     int32_t staging;        /* state: 0 global slot (L2), 1 shared memory, 2 spins in
-                               shared memory and delta energies in the global slot */
+                               shared memory and delta energies in the global slot, 3 spins
+                               and a band of delta energies around the window in shared
+                               memory, the rest in the global slot (banded problems) */
     int32_t warps_per_cta;
     int32_t ctas_per_sm;
     int32_t registers;      /* register budget per thread of the chosen kernel */

@@ -192,6 +192,57 @@ def test_in_window_resolution_shared_stream_and_odd_spins(gibbs):
     np.testing.assert_array_equal(bits(e), bits(want_e))
 
 
+# ---- banded problems (delta energies of a band around the window on chip) --
+
+def _banded_problem(rng, n, width, long_frac):
+    """Couplers between variables at most `width` apart, plus a fraction of
+    long-range ones (those stay in the global slot)."""
+    u = rng.integers(0, n - 1, 3 * n)
+    v = np.minimum(u + rng.integers(1, width + 1, u.shape[0]), n - 1)
+    far = rng.random(u.shape[0]) < long_frac
+    v[far] = rng.integers(0, n, int(far.sum()))
+    keep = u != v
+    u, v = np.minimum(u[keep], v[keep]), np.maximum(u[keep], v[keep])
+    J = rng.normal(0, 1, u.shape[0])
+    h = rng.normal(0, 0.1, n)
+    return h, u.astype(np.int32), v.astype(np.int32), J
+
+
+@pytest.mark.parametrize("gibbs", [False, True])
+def test_banded_problem_vs_oracle(gibbs):
+    """n = 12000 with couplings mostly within 60 positions: above the on-chip
+    size, so the call keeps a band of delta energies around the window in
+    shared memory and the rest in the global slot; the band slides every pass
+    and is written back and reloaded every sweep."""
+    rng = np.random.default_rng(41 + gibbs)
+    n = 12000
+    h, u, v, J = _banded_problem(rng, n, 60, 0.02)
+    betas = np.geomspace(0.05, 4.0, 12)
+    crit = "Gibbs" if gibbs else "Metropolis"
+    st = (2 * rng.integers(0, 2, (24, n)) - 1).astype(np.int8)
+    st[5, :7] = 3  # spins other than +-1
+    seeds = np.arange(24, dtype=np.uint64) + 900
+    stats = {}
+    s, e = simulated_annealing(24, h, u, v, J, 1, betas, 0, st.copy(), False, crit, seeds=seeds,
+                               stats=stats)
+    assert stats["near_ties"] == 0
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(r):
+        return oracle.run(h, u, v, J, st[r:r + 1], 1, betas, seeds[r:r + 1], False, gibbs)
+    with ThreadPoolExecutor(8) as ex:
+        want = list(ex.map(one, range(24)))
+    for r, (ws, we) in enumerate(want):
+        np.testing.assert_array_equal(s[r], ws[0])
+        assert bits(e[r:r + 1])[0] == bits(we)[0]
+    # one RNG stream continued across reads (one warp)
+    ws, we = oracle.run(h, u, v, J, st[:3], 1, betas, [77], False, gibbs)
+    s2, e2 = simulated_annealing(3, h, u, v, J, 1, betas, 77, st[:3].copy(), False, crit,
+                                 rng_stream="shared")
+    np.testing.assert_array_equal(s2, ws)
+    np.testing.assert_array_equal(bits(e2), bits(we))
+
+
 # ---- tests/test_simulated_annealing.py restated against the CUDA path -------
 
 def fm_problem(num_variables=10, num_samples=100, num_sweeps=1000):

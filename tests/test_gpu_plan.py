@@ -256,3 +256,40 @@ def test_sharded_batch_on_two_host_threads_equals_one_call():
     for pa, pb, xa, xb in zip(a, b, ea, eb):
         np.testing.assert_array_equal(pa.states, pb.states)
         np.testing.assert_array_equal(bits(xa), bits(xb))
+
+
+def test_band_location_in_every_register_budget(tmp_path):
+    """A banded problem run with the band location forced through the tuning
+    cache, in each register budget, reproduces the untuned run; problems that
+    are not banded fall back to another location."""
+    rng = np.random.default_rng(3)
+    n = 10000
+    u = rng.integers(0, n - 1, 3 * n)
+    v = np.minimum(u + rng.integers(1, 50, u.shape[0]), n - 1)
+    keep = u != v
+    u, v = np.minimum(u[keep], v[keep]).astype(np.int32), np.maximum(u[keep], v[keep]).astype(np.int32)
+    band = Instance(rng.normal(0, 0.1, n), u, v, rng.normal(0, 1, u.shape[0]),
+                    random_states(rng, 12, n), np.geomspace(0.1, 3.0, 6), 1,
+                    np.arange(12, dtype=np.uint64) + 5)
+    probs = [band] + mixed_batch(seed=59)[:3]
+    cache = tmp_path / "tune.txt"
+    with Plan(probs) as plan:
+        sin, ref, en_ref = device_buffers(plan, probs)
+        plan.run(sin, ref, en_ref, mode="plain")
+        plan.autotune(str(cache), force=True)
+        out = torch.empty_like(ref)
+        en = torch.empty_like(en_ref)
+        plan.run(sin, out, en)
+        assert torch.equal(out, ref) and torch.equal(en, en_ref)
+    keys = [line.split()[0] for line in cache.read_text().splitlines()]
+    for regs in (0, 1, 2):
+        cache.write_text("".join(f"{k} 3 2 0 {regs} 1.0\n" for k in keys))
+        with Plan(probs) as plan:
+            plan.autotune(str(cache))
+            for mode in ("persistent", "plain_tuned"):
+                out = torch.empty_like(ref)
+                en = torch.empty_like(en_ref)
+                plan.run(sin, out, en, mode=mode)
+                assert torch.equal(out, ref) and torch.equal(en, en_ref), (regs, mode)
+            rep = plan.bucket_report()
+            assert any(r["staging"] == 3 for r in rep)
