@@ -326,12 +326,14 @@ __device__ __forceinline__ bool load_state(const ProblemDev *PD, const int8_t *s
 // `s_old` (valid on flipping lanes).  The flipping variables must be pairwise
 // non-adjacent.  Entries are applied lane-parallel in rounds of 32; equal
 // targets within a round are summed in entry order by their first lane.
-// `scratch` holds 32 doubles followed by 32 ints.
+// `scratch` holds 32 doubles followed by 32 ints.  With `own_fresh`, no entry
+// of this pass names the lane's own slot, which then still holds `d_own`.
 template <class DE>
 __device__ __forceinline__ void apply_flips(const Prob &P, DE de, int8_t *sp,
                                             double *scratch, unsigned fm, int v,
                                             int start, int deg, int s_old,
-                                            bool may_conflict, unsigned lane) {
+                                            bool may_conflict, unsigned lane,
+                                            bool own_fresh = false, double d_own = 0.0) {
     const bool f = (fm >> lane) & 1u;
     const double mult = (double)(int)(int8_t)(4 * s_old);
     int *owner_of_rank = reinterpret_cast<int *>(scratch + 32);
@@ -399,7 +401,7 @@ __device__ __forceinline__ void apply_flips(const Prob &P, DE de, int8_t *sp,
     }
     if (f) {  // cpu_sa.cpp:189-190, after the variable's own updates
         sp[v] = (int8_t)(-s_old);
-        de[v] = __dmul_rn(de[v], -1.0);
+        de[v] = __dmul_rn(own_fresh ? d_own : de[v], -1.0);
     }
     __syncwarp();
 }
@@ -776,6 +778,12 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                     const bool f = (fm >> lane) & 1u;
                     const bool may_conflict =
                         __any_sync(kFull, f && ((shr & 1u) || ((shr >> 1) & later)));
+                    // Without resolution the committed flips are pairwise
+                    // non-adjacent, so a flip's own slot receives an addition
+                    // in this pass only from a repeated target in its own
+                    // list; otherwise it still holds the window value d and
+                    // the negation needs no load.
+                    const bool own_fresh = !resolve && !(shr & 1u);
                     if (D) {
                         if (!pre) {
                             if (f) rank_tab[__popc(fm & lt_mask)] = (int)lane;
@@ -786,12 +794,13 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                                        (double)(int)(int8_t)(4 * s_cur), lane);
                         if (f) {  // cpu_sa.cpp:189-190, after the variable's own updates
                             sp[v] = (int8_t)(-s_cur);
-                            de[v] = __dmul_rn(de[v], -1.0);
+                            de[v] = __dmul_rn(own_fresh ? d : de[v], -1.0);
                         }
                         __syncwarp();
                     } else {
                         apply_flips(P, de, sp, scratch, fm, v, (int)vi.x,
-                                    (int)(vi.y & kDegMask), s_cur, may_conflict, lane);
+                                    (int)(vi.y & kDegMask), s_cur, may_conflict, lane, own_fresh,
+                                    d);
                     }
                 }
                 if constexpr (BANDED) {
