@@ -95,6 +95,8 @@ struct PackArgs {
 // the error flag and nothing is built.
 __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
     __shared__ int s_err;
+    __shared__ int s_cursor[kNoAllocMaxVars];  // next free position of each list
+    __shared__ int s_tgt[64];                  // the targets of one chunk's 64 entries
     int *err = reinterpret_cast<int *>(a.base + kOffErr);
     unsigned long long *queue = reinterpret_cast<unsigned long long *>(a.base + kOffQueue);
     int *cursor = reinterpret_cast<int *>(a.base + kOffCursor);
@@ -135,22 +137,49 @@ __global__ void __launch_bounds__(1024) noalloc_pack_kernel(PackArgs a) {
         for (int v = 0; v < a.n; ++v) {
             const int d = cursor[v];
             vinfo[v] = make_uint2((unsigned)run, (unsigned)d);
-            cursor[v] = run;
+            s_cursor[v] = run;
             run += d;
         }
     }
     __syncthreads();
-    // Fill in coupler order, one thread, so each list keeps the input order.
-    if (tid == 0) {
-        for (int64_t c = 0; c < a.m; ++c) {
-            const int u = a.cu[c], v = a.cv[c];
-            const double J = a.cw[c];
-            int k = cursor[u]++;
-            col[k] = v;
-            w[k] = J;
-            k = cursor[v]++;
-            col[k] = u;
-            w[k] = J;
+    // Fill in coupler order (each list keeps the input order, cpu_sa.cpp:
+    // 298-316), one warp, 32 couplers at a time: coupler c pushes u's entry,
+    // then v's; an entry's position is its list's cursor plus the entries of
+    // earlier couplers of the chunk (and, for v's entry of a self-loop, u's)
+    // that name the same list.
+    if (tid < 32) {
+        for (int64_t base = 0; base < a.m; base += 32) {
+            const int64_t c = base + tid;
+            const bool ok = c < a.m;
+            int u = -1, v = -2;
+            double J = 0.0;
+            if (ok) {
+                u = a.cu[c];
+                v = a.cv[c];
+                J = a.cw[c];
+            }
+            s_tgt[2 * tid] = ok ? u : -1;
+            s_tgt[2 * tid + 1] = ok ? v : -2;
+            __syncwarp();
+            if (ok) {
+                int ru = 0, rv = (u == v) ? 1 : 0;
+                for (int j = 0; j < 2 * tid; ++j) {
+                    const int t = s_tgt[j];
+                    ru += t == u;
+                    rv += t == v;
+                }
+                const int ku = s_cursor[u] + ru, kv = s_cursor[v] + rv;
+                col[ku] = v;
+                w[ku] = J;
+                col[kv] = u;
+                w[kv] = J;
+            }
+            __syncwarp();
+            if (ok) {  // the chunk's counts; every lane has read the cursors
+                atomicAdd(&s_cursor[u], 1);
+                atomicAdd(&s_cursor[v], 1);
+            }
+            __syncwarp();
         }
     }
     __syncthreads();
