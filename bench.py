@@ -37,6 +37,13 @@ from b200sa import workloads  # noqa: E402
 METRIC = "spin-flip attempts/s, 1 B200: batched vs plain (bit-exact); BM grad steps/s"
 UNIT = "attempts/s"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per attempt of the
+# n ~ 4000 bucket launch with delta energies in per-read global slots, from one
+# ncu capture of the full uneven batch with every schedule cut to 5% of its
+# sweeps: 951.8 GB over 2.26e10 attempts.  The traffic is per attempt (the
+# schedule length repeats the same sweeps), so a full launch's traffic is this
+# figure times its attempts.
+L2_SLOT_DRAM_BYTES_PER_ATTEMPT = 42.1
 
 
 def parse_args():
@@ -708,9 +715,15 @@ def run_ours(args):
     dom = max(timed_b, key=lambda b: b["attempts"]) if timed_b else None
     if dom is not None:
         achieved = dom["model_bytes"] / (dom["ms"] / 1000.0) / 1e9
+        scaled = dom["staging"] == 2 and dom["max_n"] > 2048
         line["roofline"] = {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+            "frac": achieved / peak,
+            "traffic": L2_SLOT_DRAM_BYTES_PER_ATTEMPT * dom["attempts"] if scaled else None,
+            "traffic_source": ("ncu DRAM bytes per attempt of this bucket's launch (schedules cut "
+                               "to 5%), times this launch's attempts" if scaled else
+                               "no capture for this launch's state location"),
+            "peak_source": peak_src,
             "kernel": f"sweep launch of the n<={dom['max_n']} bucket (state location "
                       f"{dom['staging']}, {dom['registers']} registers, {dom['warps_per_cta']} "
                       f"warps per CTA, grid {dom['grid']})",
