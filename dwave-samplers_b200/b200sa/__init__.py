@@ -20,4 +20,4 @@ from .simulated_annealing import per_read_seeds, simulated_annealing
 from .batch import Plan, sample_batch
 
 __all__ = ["simulated_annealing", "per_read_seeds", "sample_batch", "Plan"]
-__version__ = "0.5.0"
+__version__ = "0.6.0"

@@ -418,7 +418,7 @@ int run_persistent(b200sa_plan_s *P, LaunchArgs a, cudaStream_t st, char *err,
 
 extern "C" {
 
-const char *b200sa_version(void) { return "b200sa 0.5.0 (sm_100a)"; }
+const char *b200sa_version(void) { return "b200sa 0.6.0 (sm_100a)"; }
 
 int b200sa_check_acceptance(int64_t samples, uint64_t seed, int32_t device,
                             int64_t counts[6], char *err, size_t errlen) {

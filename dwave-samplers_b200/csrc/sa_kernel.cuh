@@ -49,16 +49,41 @@ constexpr double kTieRel = 3.552713678800501e-15;  // 2^-48
 // Stream positions are kept modulo 2^32: only their differences (all below
 // kRing) and their residues modulo kRing are used, and both survive the wrap.
 struct RingState {
-    uint64_t t0, t1;  // this lane's segment-start state for the next refill
-    uint32_t q;       // outputs consumed so far (stream position, warp-uniform)
-    uint32_t base;    // ring holds positions [base, base + kRing)
+    uint32_t q;     // outputs consumed so far (stream position, warp-uniform)
+    uint32_t base;  // ring holds positions [base, base + kRing)
 };
 
-struct Counters {
+// Per-warp words the sweep loop touches rarely, kept in the warp's shared
+// region after the conflict scratch (kColdBytes): each lane's segment-start
+// state for the next ring refill (once per kHalf draws) and the read's
+// counters (written by lane 0 once per pass).
+// Every member is accessed with 8-byte (or smaller) loads and stores, so the
+// region needs only the 8-byte alignment of the ring before it.
+struct WarpCold {
+    uint64_t seg[64];  // lane l: words 2l, 2l + 1
     unsigned long long flips;
     unsigned long long passes;
     unsigned int near;
+    unsigned int pad[3];
 };
+static_assert(sizeof(WarpCold) == kColdBytes, "cold words");
+
+// The ring is followed by the scratch (kScratchHotBytes), then WarpCold.
+__device__ __forceinline__ WarpCold *warp_cold(uint64_t *ring) {
+    return reinterpret_cast<WarpCold *>(reinterpret_cast<uint8_t *>(ring + kRing) +
+                                        kScratchHotBytes);
+}
+
+// Lane 0 adds one pass's counts to the read's counters.
+__device__ __forceinline__ void count_pass(uint64_t *ring, unsigned lane, unsigned flips,
+                                           unsigned near) {
+    if (lane == 0) {
+        WarpCold *c = warp_cold(ring);
+        c->flips += flips;
+        c->passes += 1;
+        c->near += near;
+    }
+}
 
 // ---- acceptance tests ------------------------------------------------------
 // The reference decides Metropolis as exp(x) * 2^64 > (double)rand with
@@ -129,17 +154,22 @@ __device__ __noinline__ int gibbs_exact(double d, double beta, uint64_t r) {
     return (kTwo64 > y ? 1 : 0) | (fabs(y - kTwo64) <= kTwo64 * kTieRel ? 2 : 0);
 }
 
+// A field of the problem record read again at each use (a volatile load the
+// compiler does not hoist), for values used once per sweep that are not worth
+// a register through the sweep loop.
+template <class T>
+__device__ __forceinline__ T reload(const T &x) {
+    return *reinterpret_cast<const volatile T *>(&x);
+}
+
 // Problem fields the sweep loop keeps in registers (fields used only when a
 // read starts or ends are read from the ProblemDev record there).
 struct Prob {
     int n;
-    int sweeps_per_beta;
-    int num_betas;
+    const ProblemDev *pd;  // the schedule is read from here once per beta
     const uint2 *__restrict__ vinfo;
     const int32_t *__restrict__ col;
     const double *__restrict__ w;
-    const double *__restrict__ betas;
-    const double *__restrict__ thresholds;
     const uint8_t *__restrict__ dist;
     const uint32_t *__restrict__ share;
     int regular_degree;
@@ -154,13 +184,10 @@ struct Prob {
 __device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
     Prob q;
     q.n = P->n;
-    q.sweeps_per_beta = P->sweeps_per_beta;
-    q.num_betas = P->num_betas;
+    q.pd = P;
     q.vinfo = P->vinfo;
     q.col = P->col;
     q.w = P->w;
-    q.betas = P->betas;
-    q.thresholds = P->thresholds;
     q.dist = P->dist;
     q.share = P->share;
     q.regular_degree = P->regular_degree;
@@ -173,24 +200,79 @@ __device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
     return q;
 }
 
-// Brings the line holding *p (global memory) into L1 without waiting.
+// Brings the line holding *p (global memory) into L1 / L2 without waiting.
 __device__ __forceinline__ void prefetch_l1(const void *p) {
     asm volatile("prefetch.global.L1 [%0];" : : "l"(p));
 }
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" : : "l"(p));
+}
 
-// Delta energies of a banded problem (kStageBand): the slots of the
-// variables in [lo, lo + w) live in a shared-memory ring (`b`, w a power of
-// two, slot x & (w - 1)); every other variable's slot is in the global array
-// `g`.  The band slides with the window (see sweep_sequential).  With w = 0
-// everything is global.
+// Accessors of a read's delta energies, one per state location: get, set and
+// add (de[x] = de[x] + v, rounded to nearest like the reference's `+=`,
+// cpu_sa.cpp:172-185).  kAsyncAdd: an add does not wait for memory.
+//
+// SharedDe: the warp's shared region (kStageShared).
+struct SharedDe {
+    static constexpr bool kAsyncAdd = false;
+    double *p;
+    __device__ __forceinline__ double get(int x) const { return p[x]; }
+    __device__ __forceinline__ void set(int x, double v) const { p[x] = v; }
+    __device__ __forceinline__ void add(int x, double v) const { p[x] = __dadd_rn(p[x], v); }
+};
+
+// GlobalDe: the warp's global slot (kStageGlobal, kStageSpins), L2-resident.
+// An add is a reduction performed at L2 (red.global.add.f64, round to
+// nearest even, the same rounding as a load, __dadd_rn and a store), so the
+// update phase issues its additions without waiting for the slots' values.
+// Two adds to one slot from one thread land in program order, and a barrier
+// of the warp orders them before any later access by its lanes.  Reads go to
+// L2 (ld.global.cg), where the reductions are performed, never to a line an
+// earlier read left in L1.
+struct GlobalDe {
+    static constexpr bool kAsyncAdd = true;
+    double *p;
+    __device__ __forceinline__ double get(int x) const { return __ldcg(p + x); }
+    __device__ __forceinline__ void set(int x, double v) const { __stcg(p + x, v); }
+    __device__ __forceinline__ void add(int x, double v) const {
+        asm volatile("red.global.add.f64 [%0], %1;" : : "l"(p + x), "d"(v) : "memory");
+    }
+};
+
+// BandDe: a banded problem (kStageBand).  The slots of the variables in
+// [lo, lo + w) live in a shared-memory ring (`b`, w a power of two, slot
+// x & (w - 1)); every other variable's slot is in the global array `g`.  The
+// band slides with the window (see sweep_sequential) and fetches its slots
+// with cp.async through L1, so the global part is read and written with plain
+// loads and stores.  With w = 0 everything is global.
 struct BandDe {
+    static constexpr bool kAsyncAdd = false;
     double *g;
     double *b;
     int lo;
     unsigned w;
-    __device__ __forceinline__ double &operator[](int x) const {
+    __device__ __forceinline__ double &at(int x) const {
         return (unsigned)(x - lo) < w ? b[(unsigned)x & (w - 1u)] : g[x];
     }
+    __device__ __forceinline__ double get(int x) const { return at(x); }
+    __device__ __forceinline__ void set(int x, double v) const { at(x) = v; }
+    __device__ __forceinline__ void add(int x, double v) const {
+        double &s = at(x);
+        s = __dadd_rn(s, v);
+    }
+};
+
+template <int STAGE>
+struct DeFor {
+    using T = GlobalDe;
+};
+template <>
+struct DeFor<kStageShared> {
+    using T = SharedDe;
+};
+template <>
+struct DeFor<kStageBand> {
+    using T = BandDe;
 };
 
 // 8-byte asynchronous copy global -> shared (completes at cp_async_wait).
@@ -258,24 +340,26 @@ __device__ __forceinline__ void ring_init(uint64_t *ring, RingState &rs,
     xs_jump(s0, s1);
     ring_fill(ring, kHalf, s0, s1, lane);
     xs_jump(s0, s1);
-    rs.t0 = s0;
-    rs.t1 = s1;
+    uint64_t *seg = warp_cold(ring)->seg + 2 * lane;
+    seg[0] = s0;
+    seg[1] = s1;
     rs.q = 0;
     rs.base = 0;
     __syncwarp();
 }
 
 // Overwrites the consumed lower half with the positions kRing further on and
-// returns this lane's next segment-start state.  Out of line: it runs once per
+// advances this lane's segment-start state.  Out of line: it runs once per
 // kHalf draws.
-__device__ __noinline__ ulonglong2 ring_refill_half(uint64_t *ring, uint32_t pos,
-                                                    ulonglong2 t, unsigned lane) {
+__device__ __noinline__ void ring_refill_half(uint64_t *ring, uint32_t pos, unsigned lane) {
     __syncwarp();
-    ring_fill(ring, pos, t.x, t.y, lane);
-    uint64_t s0 = t.x, s1 = t.y;
+    uint64_t *seg = warp_cold(ring)->seg + 2 * lane;
+    uint64_t s0 = seg[0], s1 = seg[1];
+    ring_fill(ring, pos, s0, s1, lane);
     xs_jump(s0, s1);
+    seg[0] = s0;
+    seg[1] = s1;
     __syncwarp();
-    return make_ulonglong2(s0, s1);
 }
 
 // Keeps positions [q, q + kHalf) available: once the lower half is consumed
@@ -283,10 +367,7 @@ __device__ __noinline__ ulonglong2 ring_refill_half(uint64_t *ring, uint32_t pos
 __device__ __forceinline__ void ring_refill(uint64_t *ring, RingState &rs,
                                             unsigned lane) {
     if (rs.q - rs.base >= (uint32_t)kHalf) {
-        const ulonglong2 t =
-            ring_refill_half(ring, rs.base + kRing, make_ulonglong2(rs.t0, rs.t1), lane);
-        rs.t0 = t.x;
-        rs.t1 = t.y;
+        ring_refill_half(ring, rs.base + kRing, lane);
         rs.base += kHalf;
     }
 }
@@ -319,6 +400,27 @@ __device__ __forceinline__ bool load_state(const ProblemDev *PD, const int8_t *s
     }
     __syncwarp();
     return pm1;
+}
+
+// The additions of entries `grp` (lanes, in entry order; values in
+// scratch) to one slot, in that order.
+template <class DE>
+__device__ __forceinline__ void add_group(const DE &de, int x, unsigned grp, const double *scratch) {
+    if constexpr (DE::kAsyncAdd) {
+        while (grp) {
+            const int j = __ffs(grp) - 1;
+            grp &= grp - 1;
+            de.add(x, scratch[j]);
+        }
+    } else {
+        double acc = de.get(x);
+        while (grp) {
+            const int j = __ffs(grp) - 1;
+            grp &= grp - 1;
+            acc = __dadd_rn(acc, scratch[j]);
+        }
+        de.set(x, acc);
+    }
 }
 
 // cpu_sa.cpp:168-191 for every lane whose bit is set in `fm`.  Lane k of
@@ -355,6 +457,46 @@ __device__ __forceinline__ void apply_flips(const Prob &P, DE de, int8_t *sp,
         excl = incl - my;
         total = __shfl_sync(kFull, incl, 31);
     }
+    if (!may_conflict && !D) {
+        // No two entries name the same slot: each chunk of 96 entries issues
+        // all of its delta-energy loads before its stores.
+        for (int base = 0; base < total; base += 96) {
+            int nb[3];
+            double x[3], dv[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                const int t = base + 32 * i + (int)lane;
+                int k = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const int ex = __shfl_sync(kFull, excl, k + step);
+                    if (ex <= t) k += step;
+                }
+                const int e = __shfl_sync(kFull, start, k) + (t - __shfl_sync(kFull, excl, k));
+                const double m_k = __shfl_sync(kFull, mult, k);
+                nb[i] = 0;
+                x[i] = 0.0;
+                if (t < total) {
+                    nb[i] = __ldg(&P.col[e]);
+                    x[i] = __dmul_rn(__dmul_rn(m_k, __ldg(&P.w[e])), (double)(int)sp[nb[i]]);
+                }
+            }
+            if constexpr (DE::kAsyncAdd) {
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    if (base + 32 * i + (int)lane < total) de.add(nb[i], x[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    if (base + 32 * i + (int)lane < total) dv[i] = de.get(nb[i]);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    if (base + 32 * i + (int)lane < total) de.set(nb[i], __dadd_rn(dv[i], x[i]));
+            }
+        }
+        __syncwarp();
+        total = 0;  // done
+    }
     for (int base = 0; base < total; base += 32) {
         const int t = base + (int)lane;
         const bool a = t < total;
@@ -382,65 +524,108 @@ __device__ __forceinline__ void apply_flips(const Prob &P, DE de, int8_t *sp,
         }
         const unsigned grp = may_conflict ? __match_any_sync(kFull, nb) : (1u << lane);
         const bool alone = grp == (1u << lane);
-        if (a && alone) de[nb] = __dadd_rn(de[nb], x);
+        if (a && alone) de.add(nb, x);
         if (may_conflict && __any_sync(kFull, a && !alone)) {
             scratch[lane] = x;
             __syncwarp();
             if (a && !alone && lane == (unsigned)(__ffs(grp) - 1)) {
-                double acc = de[nb];
-                unsigned g = grp;
-                while (g) {
-                    const int j = __ffs(g) - 1;
-                    g &= g - 1;
-                    acc = __dadd_rn(acc, scratch[j]);
-                }
-                de[nb] = acc;
+                add_group(de, nb, grp, scratch);
             }
         }
         __syncwarp();
     }
     if (f) {  // cpu_sa.cpp:189-190, after the variable's own updates
         sp[v] = (int8_t)(-s_old);
-        de[v] = __dmul_rn(own_fresh ? d_own : de[v], -1.0);
+        de.set(v, __dmul_rn(own_fresh ? d_own : de.get(v), -1.0));
     }
     __syncwarp();
 }
 
-// Neighbour updates of the committed flips for equal-length lists (D entries
-// each, list v at v * D).  `rank_tab[f]` is the lane of the f-th committed
-// flip in variable order; `mult` is each lane's (int8)(4 * s) as a double
-// (cpu_sa.cpp:172), read by the entry's owner lane.  With `pre`, the entries
-// of the first 64 accepted flips were loaded into (nb0, w0, k0) / (nb1, w1,
-// k1) before the commit point was known (the committed flips are then a
-// prefix of the accepted ones); the other entries are loaded here.  Equal
-// targets within a round are summed in entry order by their first lane, as in
-// apply_flips.
-template <class DE>
-__device__ __forceinline__ void update_regular(const Prob &P, DE de, int8_t *sp,
-                                               double *scratch, const int *rank_tab,
-                                               int nflips, int p, bool pre, int nb0, double w0,
-                                               int k0, int nb1, double w1, int k1,
-                                               bool may_conflict, double mult, unsigned lane) {
+// Adjacency entries t = 32 i + lane (i < kPreGroups) of the accepted flips'
+// lists in flip order, loaded before the commit point is known: target,
+// coupling and the lane of the entry's flip.
+constexpr int kPreGroups = 2;
+struct PreEntries {
+    int nb[kPreGroups];
+    int k[kPreGroups];
+    double w[kPreGroups];
+};
+
+// Entry t of the flips' lists for equal-length lists (list v at v * D): its
+// target, coupling and the lane k of its flip.  `rank_tab[f]` is the lane of
+// the f-th flip in variable order.
+__device__ __forceinline__ void regular_load(const Prob &P, const int *rank_tab, int p, int t,
+                                             int &k, int &nb, double &wt) {
     const int D = P.regular_degree;
-    const int total = nflips * D;
+    const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);  // t / D
+    k = rank_tab[r];
+    const int e = (p + k) * D + (t - r * D);
+    nb = __ldg(&P.col[e]);
+    wt = __ldg(&P.w[e]);
+}
+
+// Neighbour updates of the committed flips for equal-length lists.  `mult` is
+// each lane's (int8)(4 * s) as a double (cpu_sa.cpp:172), read from the
+// entry's owner lane.  With `pre`, the first 32 kPreGroups entries are in `pe`
+// (loaded when only the accepted flips were known; the committed flips are a
+// prefix of them); the other entries are loaded here.
+//
+// When no two entries of the pass can name the same slot, the entries go in
+// chunks of 32 kPreGroups whose delta-energy loads are all issued before
+// their stores, so a chunk waits on memory once.  Otherwise they go in rounds
+// of 32, equal targets within a round summed in entry order by their first
+// lane, as in apply_flips.
+template <class DE>
+__device__ __forceinline__ void update_regular(const Prob &P, DE de, const int8_t *sp,
+                                               double *scratch, const int *rank_tab,
+                                               int nflips, int p, bool pre, const PreEntries &pe,
+                                               bool may_conflict, double mult, unsigned lane) {
+    const int total = nflips * P.regular_degree;
+    if (!may_conflict) {
+        for (int base = 0; base < total; base += 32 * kPreGroups) {
+            int nb[kPreGroups];
+            double x[kPreGroups], dv[kPreGroups];
+#pragma unroll
+            for (int i = 0; i < kPreGroups; ++i) {
+                const int t = base + 32 * i + (int)lane;
+                int k = 0, q = 0;
+                double wt = 0.0;
+                if (pre && base == 0) {
+                    k = pe.k[i], q = pe.nb[i], wt = pe.w[i];
+                } else if (t < total) {
+                    regular_load(P, rank_tab, p, t, k, q, wt);
+                }
+                const double m_k = __shfl_sync(kFull, mult, k);
+                nb[i] = q;
+                x[i] = __dmul_rn(__dmul_rn(m_k, wt), (double)(int)sp[q]);
+            }
+            if constexpr (DE::kAsyncAdd) {
+#pragma unroll
+                for (int i = 0; i < kPreGroups; ++i)
+                    if (base + 32 * i + (int)lane < total) de.add(nb[i], x[i]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < kPreGroups; ++i)
+                    if (base + 32 * i + (int)lane < total) dv[i] = de.get(nb[i]);
+#pragma unroll
+                for (int i = 0; i < kPreGroups; ++i)
+                    if (base + 32 * i + (int)lane < total) de.set(nb[i], __dadd_rn(dv[i], x[i]));
+            }
+        }
+        __syncwarp();
+        return;
+    }
     for (int base = 0; base < total; base += 32) {
         const int t = base + (int)lane;
         const bool a = t < total;
-        int k, nb;
-        double wt;
+        int k = 0, nb = 0;
+        double wt = 0.0;
         if (pre && base == 0) {
-            k = k0, nb = nb0, wt = w0;
+            k = pe.k[0], nb = pe.nb[0], wt = pe.w[0];
         } else if (pre && base == 32) {
-            k = k1, nb = nb1, wt = w1;
-        } else {
-            k = 0, nb = 0, wt = 0.0;
-            if (a) {
-                const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
-                k = rank_tab[r];
-                const int e = (p + k) * D + (t - r * D);
-                nb = __ldg(&P.col[e]);
-                wt = __ldg(&P.w[e]);
-            }
+            k = pe.k[1], nb = pe.nb[1], wt = pe.w[1];
+        } else if (a) {
+            regular_load(P, rank_tab, p, t, k, nb, wt);
         }
         const double m_k = __shfl_sync(kFull, mult, k);
         double x = 0.0;
@@ -449,21 +634,14 @@ __device__ __forceinline__ void update_regular(const Prob &P, DE de, int8_t *sp,
         } else {
             nb = -1 - (int)lane;  // distinct per inactive lane
         }
-        const unsigned grp = may_conflict ? __match_any_sync(kFull, nb) : (1u << lane);
+        const unsigned grp = __match_any_sync(kFull, nb);
         const bool alone = grp == (1u << lane);
-        if (a && alone) de[nb] = __dadd_rn(de[nb], x);
-        if (may_conflict && __any_sync(kFull, a && !alone)) {
+        if (a && alone) de.add(nb, x);
+        if (__any_sync(kFull, a && !alone)) {
             scratch[lane] = x;
             __syncwarp();
             if (a && !alone && lane == (unsigned)(__ffs(grp) - 1)) {
-                double acc = de[nb];
-                unsigned g = grp;
-                while (g) {
-                    const int j = __ffs(g) - 1;
-                    g &= g - 1;
-                    acc = __dadd_rn(acc, scratch[j]);
-                }
-                de[nb] = acc;
+                add_group(de, nb, grp, scratch);
             }
         }
         __syncwarp();
@@ -490,7 +668,7 @@ __device__ __forceinline__ void update_dense(const Prob &P, DE de, int8_t *sp,
         dx[i] = 0.0;
         sx[i] = 0.0;
         if (x < n) {
-            dx[i] = de[x];
+            dx[i] = de.get(x);
             sx[i] = (double)(int)sp[x];
         }
     }
@@ -515,11 +693,11 @@ __device__ __forceinline__ void update_dense(const Prob &P, DE de, int8_t *sp,
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
-        if ((touched >> i) & 1u) de[(int)lane + 32 * i] = dx[i];
+        if ((touched >> i) & 1u) de.set((int)lane + 32 * i, dx[i]);
     __syncwarp();
     if ((fm >> lane) & 1u) {  // cpu_sa.cpp:189-190, after the variable's own updates
         sp[v] = (int8_t)(-s_cur);
-        de[v] = __dmul_rn(de[v], -1.0);
+        de.set(v, __dmul_rn(de.get(v), -1.0));
     }
     __syncwarp();
 }
@@ -566,39 +744,33 @@ __device__ __forceinline__ int decide(double d, double beta, uint64_t r) {
 // window live in a shared-memory ring of band_w slots (BandDe), the rest in
 // the global slot `de_g`.  After each pass the band slides by the committed
 // count: the slots leaving it are written back and the ones entering are
-// fetched asynchronously; band_w >= 2 band_b + 128 keeps every fetch at least
-// two passes ahead of its first use (cp.async.wait_group 1 at each pass).  At
-// every sweep the band is written back and reloaded from the start.
-template <bool BANDED>
-struct DeSel {
-    using T = double *;
-};
-template <>
-struct DeSel<true> {
-    using T = BandDe;
-};
-
-template <bool GIBBS, bool DENSE_OK, bool BANDED>
+// fetched asynchronously.  band_w >= 2 band_b + 128 keeps the slots fetched
+// by a slide at least four passes ahead of the window, so every pass waits
+// only for the slides before the last one (cp.async.wait_group 1) before its
+// decisions read the window; an update through a coupler longer than band_b
+// can reach the last slide's slots, so the update phase waits for all of
+// them.  At every sweep the band is written back and reloaded from the start.
+template <bool GIBBS, bool DENSE_OK, int STAGE>
 __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                                                  int8_t *sp, double *scratch,
                                                  uint64_t *ring, RingState &rs,
-                                                 unsigned lane, Counters &cnt,
-                                                 bool resolve, bool de_global, double *band,
-                                                 int band_w, int band_b) {
+                                                 unsigned lane, bool resolve,
+                                                 double *band, int band_w, int band_b) {
+    constexpr bool BANDED = STAGE == kStageBand;
     const int n = P.n;
     const int D = P.regular_degree;
     const unsigned lt_mask = (1u << lane) - 1u;
     int *rank_tab = reinterpret_cast<int *>(scratch + 32);
-    typename DeSel<BANDED>::T de;
+    typename DeFor<STAGE>::T de;
     bool band_live = false;
     if constexpr (BANDED)
         de = BandDe{de_g, band, 0, (unsigned)band_w};
     else
-        de = de_g;
-    for (int b = 0; b < P.num_betas; ++b) {
-        const double beta = __ldg(&P.betas[b]);
-        const double thr = __ldg(&P.thresholds[b]);
-        for (int sw = 0; sw < P.sweeps_per_beta; ++sw) {
+        de.p = de_g;
+    for (int b = 0; b < reload(P.pd->num_betas); ++b) {
+        const double beta = __ldg(&reload(P.pd->betas)[b]);
+        const double thr = __ldg(&reload(P.pd->thresholds)[b]);
+        for (int sw = 0; sw < reload(P.pd->sweeps_per_beta); ++sw) {
             if constexpr (BANDED) {
                 if (band_w) {  // write the band back, reload it at the start
                     cp_async_wait<0>();
@@ -637,14 +809,12 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                 uint2 bk = make_uint2(0u, 0u);
                 int s_cur = 0;
                 if (act) {
-                    d = de[v];
+                    d = de.get(v);
                     dist = __ldg(&P.dist[v]);
                     shr = __ldg(&P.share[v]);
                     if (!D) vi = __ldg(&P.vinfo[v]);
-                    if (resolve) {
-                        bk = __ldg(&P.back[v]);
-                        s_cur = (int)sp[v];
-                    }
+                    if (resolve) bk = __ldg(&P.back[v]);
+                    s_cur = (int)sp[v];
                 }
                 // The nearest back neighbour's coupling (stored last), loaded
                 // ahead: on lattices and chains it is the one the rounds need.
@@ -663,7 +833,8 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                         prefetch_l1(P.dist + vn);
                         prefetch_l1(P.share + vn);
                         if (!D) prefetch_l1(P.vinfo + vn);
-                        if (!BANDED && de_global) prefetch_l1(de_g + vn);
+                        // Global slots are read from L2 (GlobalDe).
+                        if constexpr (DeFor<STAGE>::T::kAsyncAdd) prefetch_l2(de_g + vn);
                         if (resolve) prefetch_l1(P.back + vn);
                     }
                     if (resolve) {  // the update phase's lists (no early load with resolution)
@@ -688,26 +859,18 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                 // adjacency before the commit point is known (not with
                 // resolution, whose later rounds change the accepted set).
                 const bool pre = !resolve;
-                int nb0 = 0, nb1 = 0, k0 = 0, k1 = 0;
-                double w0 = 0.0, w1 = 0.0;
+                const double mult = (double)(int)(int8_t)(4 * s_cur);
+                PreEntries pe;
+#pragma unroll
+                for (int i = 0; i < kPreGroups; ++i) pe.nb[i] = 0, pe.k[i] = 0, pe.w[i] = 0.0;
                 if (D && am && pre) {
                     if (acc) rank_tab[__popc(am & lt_mask)] = (int)lane;
                     __syncwarp();
-                    const int pre_n = min(__popc(am) * D, 64);
-                    if ((int)lane < pre_n) {
-                        const int r = (int)((lane * P.regular_magic) >> 16);
-                        k0 = rank_tab[r];
-                        const int e = (p + k0) * D + ((int)lane - r * D);
-                        nb0 = __ldg(&P.col[e]);
-                        w0 = __ldg(&P.w[e]);
-                    }
-                    if ((int)lane + 32 < pre_n) {
-                        const int t = (int)lane + 32;
-                        const int r = (int)(((uint32_t)t * P.regular_magic) >> 16);
-                        k1 = rank_tab[r];
-                        const int e = (p + k1) * D + (t - r * D);
-                        nb1 = __ldg(&P.col[e]);
-                        w1 = __ldg(&P.w[e]);
+                    const int pre_n = min(__popc(am) * D, 32 * kPreGroups);
+#pragma unroll
+                    for (int i = 0; i < kPreGroups; ++i) {
+                        const int t = (int)lane + 32 * i;
+                        if (t < pre_n) regular_load(P, rank_tab, p, t, pe.k[i], pe.nb[i], pe.w[i]);
                     }
                 }
                 const int bound = acc ? (int)lane + dist : 32;
@@ -722,56 +885,67 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                     const unsigned smask = __ballot_sync(kFull, s_cur > 0);
                     const double sk = (double)s_cur;
                     unsigned newf = fm;
+                    // Each lane keeps the flags of its latest decision; a
+                    // committed lane's are final, so the ballots of a round
+                    // cover the committed lanes too (its draw position counts
+                    // the committed draws before it).
+                    bool need_l = need, acc_l = acc;
+                    unsigned nm_all;
                     do {
-                        if (act && (int)lane >= c) {
-                            unsigned rel = back_lanes & newf;
-                            while (rel) {
-                                const int j = __ffs(rel) - 1;
-                                rel &= rel - 1u;
-                                const int o = (int)lane - j;
-                                // Offsets are stored descending: o's rank
-                                // is the number of larger offsets.
-                                const int rank = __popcll((unsigned long long)bk.x >> (o + 1));
-                                const double wj =
-                                    o == o_near ? bw_near : __ldg(&P.bw[bk.y + (uint32_t)rank]);
-                                const double mj = ((smask >> j) & 1u) ? 4.0 : -4.0;
-                                d = __dadd_rn(d, __dmul_rn(__dmul_rn(mj, wj), sk));
-                            }
-                        }
                         const bool live = act && (int)lane >= c;
-                        const bool cons2 = live && !(d >= thr);
-                        const bool need2 = GIBBS ? cons2 : (cons2 && !(d <= 0.0));
-                        const unsigned nm2 = __ballot_sync(kFull, need2);
-                        bool acc2 = GIBBS ? false : cons2;
-                        bool near2 = false;
-                        if (need2) {
-                            const uint64_t r =
-                                ring[(rs.q + used + (uint32_t)__popc(nm2 & lt_mask)) & (kRing - 1)];
-                            const int x = decide<GIBBS>(d, beta, r);
-                            acc2 = (x & 1) != 0;
-                            near2 = (x & 2) != 0;
+                        unsigned rel = live ? back_lanes & newf : 0u;
+                        while (rel) {
+                            const int j = __ffs(rel) - 1;
+                            rel &= rel - 1u;
+                            const int o = (int)lane - j;
+                            double wj = bw_near;
+                            if (o != o_near) {
+                                // Offsets are stored descending: o's rank is
+                                // the number of larger offsets.
+                                wj = __ldg(&P.bw[bk.y + (uint32_t)__popc((bk.x >> o) >> 1)]);
+                            }
+                            const double mj = ((smask >> j) & 1u) ? 4.0 : -4.0;
+                            d = __dadd_rn(d, __dmul_rn(__dmul_rn(mj, wj), sk));
                         }
-                        const unsigned am2 = __ballot_sync(kFull, acc2);
-                        const int bound2 = acc2 ? (int)lane + dist : 32;
+                        if (live) {
+                            const bool cons2 = !(d >= thr);
+                            need_l = GIBBS ? cons2 : (cons2 && !(d <= 0.0));
+                            acc_l = GIBBS ? false : cons2;
+                            near = false;
+                        }
+                        nm_all = __ballot_sync(kFull, need_l);
+                        if (live && need_l) {
+                            const uint64_t r =
+                                ring[(rs.q + (uint32_t)__popc(nm_all & lt_mask)) & (kRing - 1)];
+                            const int x = decide<GIBBS>(d, beta, r);
+                            acc_l = (x & 1) != 0;
+                            near = (x & 2) != 0;
+                        }
+                        const unsigned am_all = __ballot_sync(kFull, acc_l);
+                        const int bound2 = (live && acc_l) ? (int)lane + dist : 32;
                         c = min(__reduce_min_sync(kFull, bound2), L);
                         const unsigned upto = c >= 32 ? kFull : ((1u << c) - 1u);
-                        const unsigned commit2 = upto & ~done;
-                        used += (uint32_t)__popc(nm2 & commit2);
-                        nearm |= __ballot_sync(kFull, near2) & commit2;
-                        newf = am2 & commit2;
-                        fm |= newf;
+                        newf = am_all & upto & ~done;
+                        fm = am_all & upto;
                         done = upto;
                     } while (c < L);
+                    used = (uint32_t)__popc(nm_all & done);
+                    nearm = __ballot_sync(kFull, near) & done;
                 }
                 rs.q += used;
-                cnt.near += __popc(nearm);
-                cnt.flips += __popc(fm);
-                cnt.passes += 1;
+                count_pass(ring, lane, (unsigned)__popc(fm), (unsigned)__popc(nearm));
+                if constexpr (BANDED) {
+                    // The slots the last slide fetched lie at the far end of
+                    // the band, which only an update through a coupler longer
+                    // than band_b can reach: they land before the update phase.
+                    if (band_w && fm) {
+                        cp_async_wait<0>();
+                        __syncwarp();
+                    }
+                }
                 if (fm && DENSE_OK && P.dense) {
-                    if (!resolve) s_cur = act ? (int)sp[v] : 0;
                     update_dense(P, de, sp, fm, p, v, s_cur, lane);
                 } else if (fm) {
-                    if (!resolve) s_cur = act ? (int)sp[v] : 0;
                     // A slot can receive two additions only through a repeated
                     // target in one list or a neighbour common to two flips.
                     const unsigned later = lane < 31 ? fm >> (lane + 1) : 0u;
@@ -789,12 +963,11 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                             if (f) rank_tab[__popc(fm & lt_mask)] = (int)lane;
                             __syncwarp();
                         }
-                        update_regular(P, de, sp, scratch, rank_tab, __popc(fm), p, pre, nb0, w0,
-                                       k0, nb1, w1, k1, may_conflict,
-                                       (double)(int)(int8_t)(4 * s_cur), lane);
+                        update_regular(P, de, sp, scratch, rank_tab, __popc(fm), p, pre, pe,
+                                       may_conflict, mult, lane);
                         if (f) {  // cpu_sa.cpp:189-190, after the variable's own updates
                             sp[v] = (int8_t)(-s_cur);
-                            de[v] = __dmul_rn(own_fresh ? d : de[v], -1.0);
+                            de.set(v, __dmul_rn(own_fresh ? d : de.get(v), -1.0));
                         }
                         __syncwarp();
                     } else {
@@ -843,24 +1016,23 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
 // in a per-warp bitmap (`touch`, n bits, clear between passes).  Committed
 // flips are pairwise distinct and non-adjacent, so their neighbour updates
 // are applied together, equal targets summed in entry order.
-template <bool GIBBS>
-__device__ __forceinline__ void sweep_random(const Prob &P, double *de,
+template <bool GIBBS, class DE>
+__device__ __forceinline__ void sweep_random(const Prob &P, DE de,
                                              int8_t *sp, double *scratch,
                                              uint64_t *ring, RingState &rs,
-                                             unsigned lane, Counters &cnt,
-                                             uint32_t *touch) {
+                                             unsigned lane, uint32_t *touch) {
     const int n = P.n;
     const int D = P.regular_degree;
-    for (int b = 0; b < P.num_betas; ++b) {
-        const double beta = __ldg(&P.betas[b]);
-        const double thr = __ldg(&P.thresholds[b]);
-        for (int sw = 0; sw < P.sweeps_per_beta; ++sw) {
+    for (int b = 0; b < reload(P.pd->num_betas); ++b) {
+        const double beta = __ldg(&reload(P.pd->betas)[b]);
+        const double thr = __ldg(&reload(P.pd->thresholds)[b]);
+        for (int sw = 0; sw < reload(P.pd->sweeps_per_beta); ++sw) {
             int rem = n;  // attempts left in this sweep
             while (rem > 0) {
                 ring_refill(ring, rs, lane);
                 const uint64_t rv = ring[(rs.q + lane) & (kRing - 1)];
                 const int var = (int)(rv % (uint64_t)n);  // cpu_sa.cpp:135-136
-                const double d = de[var];
+                const double d = de.get(var);
                 const bool cons = !(d >= thr);            // cpu_sa.cpp:140
                 const bool need = GIBBS ? cons : (cons && !(d <= 0.0));
                 const unsigned N = __ballot_sync(kFull, need);
@@ -936,9 +1108,8 @@ __device__ __forceinline__ void sweep_random(const Prob &P, double *de,
                 rs.q += (uint32_t)(last + 1) + ((N >> last) & 1u);
                 rem -= __popc(cm);
                 const unsigned fm = A & cm;
-                cnt.near += __popc(__ballot_sync(kFull, near) & cm);
-                cnt.flips += __popc(fm);
-                cnt.passes += 1;
+                count_pass(ring, lane, (unsigned)__popc(fm),
+                           (unsigned)__popc(__ballot_sync(kFull, near) & cm));
                 if (fm) {
                     const int s_old = (int)sp[var];
                     const uint2 vi = D ? make_uint2((uint32_t)var * (uint32_t)D, (uint32_t)D)
@@ -981,26 +1152,29 @@ __device__ __forceinline__ double state_energy(const ProblemDev *PD, const int8_
     return e;
 }
 
-template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE, bool BANDED>
+template <bool GIBBS, bool RANDOM_ORDER, bool RESOLVE, int STAGE>
 __device__ __forceinline__ void anneal_read(const ProblemDev *PD, const int8_t *src,
                                             int8_t *dst, double *energy_out,
                                             double *de, int8_t *sp,
                                             double *scratch, uint64_t *ring,
-                                            RingState &rs, unsigned lane,
-                                            Counters &cnt, uint32_t *touch, bool de_global,
+                                            RingState &rs, unsigned lane, uint32_t *touch,
                                             double *band, int band_cap) {
     const bool pm1 = load_state(PD, src, de, sp, lane);
     {
         const Prob P = load_prob(PD);
         if constexpr (RANDOM_ORDER) {
-            sweep_random<GIBBS>(P, de, sp, scratch, ring, rs, lane, cnt, touch);
+            static_assert(STAGE != kStageBand, "the band follows a sequential window");
+            typename DeFor<STAGE>::T acc;
+            acc.p = de;
+            sweep_random<GIBBS>(P, acc, sp, scratch, ring, rs, lane, touch);
         } else {
             // A problem whose band does not fit the launch's ring keeps all of
             // its delta energies in the global slot.
-            const int bw = (BANDED && PD->band_w > 0 && PD->band_w <= band_cap) ? PD->band_w : 0;
-            sweep_sequential<GIBBS, RESOLVE, BANDED>(P, de, sp, scratch, ring, rs, lane, cnt,
-                                                     RESOLVE && pm1, de_global, band, bw,
-                                                     PD->band_b);
+            const int bw = (STAGE == kStageBand && PD->band_w > 0 && PD->band_w <= band_cap)
+                               ? PD->band_w
+                               : 0;
+            sweep_sequential<GIBBS, RESOLVE, STAGE>(P, de, sp, scratch, ring, rs, lane,
+                                                    RESOLVE && pm1, band, bw, PD->band_b);
         }
     }
     __syncwarp();

@@ -56,8 +56,8 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
     bool stream_live = false;
     if (A.shared_stream && A.carry_in) {
         for (int i = lane; i < kRing; i += 32) ring[i] = A.rng_carry[i];
-        rs.t0 = A.rng_carry[kRing + 2 * lane];
-        rs.t1 = A.rng_carry[kRing + 2 * lane + 1];
+        warp_cold(ring)->seg[2 * lane] = A.rng_carry[kRing + 2 * lane];
+        warp_cold(ring)->seg[2 * lane + 1] = A.rng_carry[kRing + 2 * lane + 1];
         rs.q = (uint32_t)A.rng_carry[kRing + kCarryLaneWords];
         rs.base = (uint32_t)A.rng_carry[kRing + kCarryLaneWords + 1];
         stream_live = true;
@@ -82,14 +82,15 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
             stream_live = A.shared_stream != 0;
         }
         const int64_t so = PD->state_offset + (int64_t)r * PD->n;
-        Counters cnt = {0ull, 0ull, 0u};
-        anneal_read<GIBBS, RANDOM_ORDER, RESOLVE, STAGE == kStageBand>(
+        WarpCold *cold = warp_cold(ring);
+        if (lane == 0) cold->flips = 0ull, cold->passes = 0ull, cold->near = 0u;
+        anneal_read<GIBBS, RANDOM_ORDER, RESOLVE, STAGE>(
             PD, A.states_in + so, A.states_out + so, &A.energies[rd], de, sp, scratch, ring, rs,
-            lane, cnt, touch, STAGE != kStageShared, band, A.band_cap);
+            lane, touch, band, A.band_cap);
         if (lane == 0) {
-            A.stats[rd].flips = cnt.flips;
-            A.stats[rd].passes = cnt.passes;
-            A.stats[rd].near_ties = cnt.near;
+            A.stats[rd].flips = cold->flips;
+            A.stats[rd].passes = cold->passes;
+            A.stats[rd].near_ties = cold->near;
         }
         if (!A.queue_head) it += A.shared_stream ? 1 : total_warps;
     }
@@ -97,8 +98,8 @@ __device__ __forceinline__ void sa_warp_body(const LaunchArgs &A, int warps_per_
     if (A.shared_stream && stream_live) {
         __syncwarp();
         for (int i = lane; i < kRing; i += 32) A.rng_carry[i] = ring[i];
-        A.rng_carry[kRing + 2 * lane] = rs.t0;
-        A.rng_carry[kRing + 2 * lane + 1] = rs.t1;
+        A.rng_carry[kRing + 2 * lane] = warp_cold(ring)->seg[2 * lane];
+        A.rng_carry[kRing + 2 * lane + 1] = warp_cold(ring)->seg[2 * lane + 1];
         if (lane == 0) {
             A.rng_carry[kRing + kCarryLaneWords] = rs.q;
             A.rng_carry[kRing + kCarryLaneWords + 1] = rs.base;

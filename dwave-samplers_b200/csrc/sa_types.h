@@ -218,12 +218,16 @@ constexpr int kCarryLaneWords = 64;                 // 32 lanes x 2 words
 constexpr int kCarryWords = kRing + kCarryLaneWords + 2;  // ring, lanes, q, base
 
 // Per-warp shared region: RNG ring, scratch (32 doubles for equal-slot sums,
-// 32 ints for the rank table of accepted flips), delta energies, spins.
-// (region_bytes_for keeps every region a multiple of 16 bytes.)
-constexpr int kScratchBytes = 32 * 8 + 32 * 4;
+// 32 ints for the rank table of accepted flips; then the lanes' RNG
+// segment-start states and the read's counters, which the sweep loop keeps
+// out of registers), delta energies, spins.  (region_bytes_for keeps every
+// region a multiple of 16 bytes.)
+constexpr int kScratchHotBytes = 32 * 8 + 32 * 4;
+constexpr int kColdBytes = 32 * 16 + 32;
+constexpr int kScratchBytes = kScratchHotBytes + kColdBytes;
 inline int region_bytes_for(int cap_n) {
     const int spins = (cap_n + 15) & ~15;
-    return kRing * 8 + kScratchBytes + cap_n * 8 + spins;
+    return kRing * 8 + kScratchBytes + ((cap_n * 8 + 15) & ~15) + spins;
 }
 
 // Where a read's state lives: kStageGlobal keeps delta energies and spins in
