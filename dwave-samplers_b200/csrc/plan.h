@@ -153,6 +153,7 @@ struct b200sa_plan_s {
     cudaEvent_t join[b200sa::host::kStreams] = {};
     int num_problems = 0;
     int onchip_max = 0;
+    int onchip_fast = 0;  // untuned: all state on chip up to this n (24 warps' regions per SM)
     std::vector<b200sa::ProblemDev> hprobs;
     std::vector<int32_t> n, reads, sweeps;  // per problem
     std::vector<int64_t> state_off, read_off;

@@ -131,7 +131,21 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
         }
         return (int)B200SA_OK;
     };
+    // Untuned register budget: 128 registers for state on chip or in the band,
+    // the 80-register kernel (24 warps per SM) for global slots, whose delta
+    // energies are updated by L2 reductions and gain from more reads in flight.
+    bool untuned_global = false;
+    if (!(choice && choice->set) && stage == kStageShared && max_n_here > P->onchip_fast &&
+        max_n_here <= P->onchip_max &&
+        region_bytes_for_stage(kStageSpins, max_n_here) + tb <= smem_blk) {
+        // Untuned, on chip but with fewer than 24 warps' regions per SM: the
+        // spins stay in shared memory, the delta energies go to the global
+        // slot (measured faster from n ~ 1000 on).
+        stage = kStageSpins;
+        untuned_global = true;
+    }
     if (stage == kStageShared && max_n_here > P->onchip_max) {
+        untuned_global = true;
         stage = kStageGlobal;
         // Untuned, above the on-chip size, banded: the band location (spins
         // and the band of delta energies around the window on chip) when
@@ -164,7 +178,14 @@ int shape_for(b200sa_plan_s *P, int kind, int32_t max_n_here, int64_t items, boo
     const int region = region_bytes_for_stage(stage, cap, band_cap) + tb;
     out.touch_bytes = tb;
     out.band_cap = band_cap;
-    const int reg_class = choice && choice->set ? choice->reg_class : 0;
+    // (80 registers only where shared memory leaves room for more than the
+    // 16 warps per SM of the 128-register kernel.)
+    const bool more_warps =
+        17 * (region_bytes_for_stage(stage, stage == kStageGlobal ? 0 : max_n_here) + tb) +
+            2 * 1024 <= (int)P->prop.sharedMemPerMultiprocessor;
+    const int reg_class = choice && choice->set ? choice->reg_class
+                          : (untuned_global && stage != kStageBand && more_warps) ? 1
+                                                                                   : 0;
     const int variant = kernel_variant(kind, stage, reg_class);
     out.stage = stage;
     if (choice && choice->set) {
@@ -476,6 +497,12 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
             if (3 * region_bytes_for(mid) + 3 * 1024 <= smem_sm) lo = mid; else hi = mid - 1;
         }
         P->onchip_max = lo;
+        lo = 0, hi = 1 << 20;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (24 * region_bytes_for(mid) + 2 * 1024 <= smem_sm) lo = mid; else hi = mid - 1;
+        }
+        P->onchip_fast = lo;
     }
 
     // Pack and lay out every problem in one device arena.

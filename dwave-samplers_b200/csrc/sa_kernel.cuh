@@ -56,9 +56,9 @@ struct RingState {
 // Per-warp words the sweep loop touches rarely, kept in the warp's shared
 // region after the conflict scratch (kColdBytes): each lane's segment-start
 // state for the next ring refill (once per kHalf draws) and the read's
-// counters (written by lane 0 once per pass).
-// Every member is accessed with 8-byte (or smaller) loads and stores, so the
-// region needs only the 8-byte alignment of the ring before it.
+// counters (added to by lane 0 once per sweep).  Every member is accessed
+// with 8-byte (or smaller) loads and stores, so the region needs only the
+// 8-byte alignment of the ring before it.
 struct WarpCold {
     uint64_t seg[64];  // lane l: words 2l, 2l + 1
     unsigned long long flips;
@@ -74,16 +74,24 @@ __device__ __forceinline__ WarpCold *warp_cold(uint64_t *ring) {
                                         kScratchHotBytes);
 }
 
-// Lane 0 adds one pass's counts to the read's counters.
-__device__ __forceinline__ void count_pass(uint64_t *ring, unsigned lane, unsigned flips,
-                                           unsigned near) {
-    if (lane == 0) {
-        WarpCold *c = warp_cold(ring);
-        c->flips += flips;
-        c->passes += 1;
-        c->near += near;
+// One sweep's counts (warp-uniform; at most n each), added by lane 0 to the
+// read's counters when the sweep ends.
+struct SweepCount {
+    unsigned flips = 0, passes = 0, near = 0;
+    __device__ __forceinline__ void pass(unsigned f, unsigned nt) {
+        flips += f;
+        passes += 1;
+        near += nt;
     }
-}
+    __device__ __forceinline__ void flush(uint64_t *ring, unsigned lane) const {
+        if (lane == 0) {
+            WarpCold *c = warp_cold(ring);
+            c->flips += flips;
+            c->passes += passes;
+            c->near += near;
+        }
+    }
+};
 
 // ---- acceptance tests ------------------------------------------------------
 // The reference decides Metropolis as exp(x) * 2^64 > (double)rand with
@@ -154,12 +162,21 @@ __device__ __noinline__ int gibbs_exact(double d, double beta, uint64_t r) {
     return (kTwo64 > y ? 1 : 0) | (fabs(y - kTwo64) <= kTwo64 * kTieRel ? 2 : 0);
 }
 
-// A field of the problem record read again at each use (a volatile load the
-// compiler does not hoist), for values used once per sweep that are not worth
-// a register through the sweep loop.
+// A field of the problem record read again at each use, for values used once
+// per sweep that are not worth a register through the sweep loop.  The load
+// goes through the read-only cache (ld.global.nc, an L1 hit after the first
+// sweep); the asm statement is volatile so that the compiler does not hoist
+// it out of the loop.  The record does not change while a kernel runs.
+__device__ __forceinline__ int reload(const int &x) {
+    int r;
+    asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(r) : "l"(&x));
+    return r;
+}
 template <class T>
-__device__ __forceinline__ T reload(const T &x) {
-    return *reinterpret_cast<const volatile T *>(&x);
+__device__ __forceinline__ T *reload(T *const &x) {
+    unsigned long long r;
+    asm volatile("ld.global.nc.u64 %0, [%1];" : "=l"(r) : "l"(&x));
+    return reinterpret_cast<T *>(r);
 }
 
 // Problem fields the sweep loop keeps in registers (fields used only when a
@@ -771,6 +788,7 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
         const double beta = __ldg(&reload(P.pd->betas)[b]);
         const double thr = __ldg(&reload(P.pd->thresholds)[b]);
         for (int sw = 0; sw < reload(P.pd->sweeps_per_beta); ++sw) {
+            SweepCount cnt;
             if constexpr (BANDED) {
                 if (band_w) {  // write the band back, reload it at the start
                     cp_async_wait<0>();
@@ -933,7 +951,7 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                     nearm = __ballot_sync(kFull, near) & done;
                 }
                 rs.q += used;
-                count_pass(ring, lane, (unsigned)__popc(fm), (unsigned)__popc(nearm));
+                cnt.pass((unsigned)__popc(fm), (unsigned)__popc(nearm));
                 if constexpr (BANDED) {
                     // The slots the last slide fetched lie at the far end of
                     // the band, which only an update through a coupler longer
@@ -993,6 +1011,7 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                 p += c;
                 if constexpr (BANDED) de.lo = p - band_b;
             }
+            cnt.flush(ring, lane);
         }
     }
     if constexpr (BANDED) {
@@ -1027,6 +1046,7 @@ __device__ __forceinline__ void sweep_random(const Prob &P, DE de,
         const double beta = __ldg(&reload(P.pd->betas)[b]);
         const double thr = __ldg(&reload(P.pd->thresholds)[b]);
         for (int sw = 0; sw < reload(P.pd->sweeps_per_beta); ++sw) {
+            SweepCount cnt;
             int rem = n;  // attempts left in this sweep
             while (rem > 0) {
                 ring_refill(ring, rs, lane);
@@ -1108,8 +1128,7 @@ __device__ __forceinline__ void sweep_random(const Prob &P, DE de,
                 rs.q += (uint32_t)(last + 1) + ((N >> last) & 1u);
                 rem -= __popc(cm);
                 const unsigned fm = A & cm;
-                count_pass(ring, lane, (unsigned)__popc(fm),
-                           (unsigned)__popc(__ballot_sync(kFull, near) & cm));
+                cnt.pass((unsigned)__popc(fm), (unsigned)__popc(__ballot_sync(kFull, near) & cm));
                 if (fm) {
                     const int s_old = (int)sp[var];
                     const uint2 vi = D ? make_uint2((uint32_t)var * (uint32_t)D, (uint32_t)D)
@@ -1119,6 +1138,7 @@ __device__ __forceinline__ void sweep_random(const Prob &P, DE de,
                                 s_old, true, lane);
                 }
             }
+            cnt.flush(ring, lane);
         }
     }
 }
