@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -14,6 +15,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -516,9 +518,33 @@ int b200sa_plan_create(const b200sa_problem *problems, int32_t num_problems,
     };
     P->state_off.assign((size_t)num_problems + 1, 0);
     P->read_off.assign((size_t)num_problems + 1, 0);
+    // The problems' adjacency is packed on up to 32 host threads (problems
+    // are independent; each thread takes the next unpacked one).
+    {
+        const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+        const int nt = std::min(std::min(hw, 32), (int)num_problems);
+        std::atomic<int32_t> next{0};
+        std::atomic<bool> failed{false};
+        auto work = [&]() {
+            for (int32_t i; (i = next.fetch_add(1)) < num_problems;) {
+                try {
+                    pack_adjacency(problems[i], adj[i]);
+                } catch (...) {
+                    failed = true;
+                }
+            }
+        };
+        if (nt <= 1) {
+            work();
+        } else {
+            std::vector<std::thread> pool;
+            for (int t = 0; t < nt; ++t) pool.emplace_back(work);
+            for (std::thread &t : pool) t.join();
+        }
+        if (failed) return set_err(err, errlen, B200SA_ENOMEM, "out of host memory packing problems");
+    }
     for (int32_t i = 0; i < num_problems; ++i) {
         const b200sa_problem &q = problems[i];
-        pack_adjacency(q, adj[i]);
         const size_t n = (size_t)q.num_vars, m = (size_t)q.num_couplers,
                      nb = (size_t)q.num_betas;
         ArenaOffsets &o = off[i];
