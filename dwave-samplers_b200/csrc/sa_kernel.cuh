@@ -217,12 +217,9 @@ __device__ __forceinline__ Prob load_prob(const ProblemDev *P) {
     return q;
 }
 
-// Brings the line holding *p (global memory) into L1 / L2 without waiting.
+// Brings the line holding *p (global memory) into L1 without waiting.
 __device__ __forceinline__ void prefetch_l1(const void *p) {
     asm volatile("prefetch.global.L1 [%0];" : : "l"(p));
-}
-__device__ __forceinline__ void prefetch_l2(const void *p) {
-    asm volatile("prefetch.global.L2 [%0];" : : "l"(p));
 }
 
 // Accessors of a read's delta energies, one per state location: get, set and
@@ -752,10 +749,10 @@ __device__ __forceinline__ int decide(double d, double beta, uint64_t r) {
 // (a neighbour that flipped earlier) equals the negated contribution added
 // before it.
 //
-// While a window is processed, the records of the next one (and its delta
-// energies when they live in global memory) are prefetched into L1; with
-// resolution also the lines of this window's adjacency lists, which the
-// update phase reads.
+// While a window is processed, the records of the next one are prefetched
+// into L1 when the delta energies are on chip or in the band; with resolution
+// also the lines of this window's adjacency lists, which the update phase
+// reads.
 //
 // BANDED (kStageBand): the delta energies of variables within band_b of the
 // window live in a shared-memory ring of band_w slots (BandDe), the rest in
@@ -847,12 +844,12 @@ __device__ __forceinline__ void sweep_sequential(const Prob &P, double *de_g,
                     // before p + c + 32, so the lines of [v + 32] are the
                     // ones it may need beyond this window's.
                     const int vn = v + 32;
-                    if (vn < n) {
+                    // (Not with global slots: there the prefetches measured
+                    // slower than the plain loads.)
+                    if (vn < n && !DeFor<STAGE>::T::kAsyncAdd) {
                         prefetch_l1(P.dist + vn);
                         prefetch_l1(P.share + vn);
                         if (!D) prefetch_l1(P.vinfo + vn);
-                        // Global slots are read from L2 (GlobalDe).
-                        if constexpr (DeFor<STAGE>::T::kAsyncAdd) prefetch_l2(de_g + vn);
                         if (resolve) prefetch_l1(P.back + vn);
                     }
                     if (resolve) {  // the update phase's lists (no early load with resolution)

@@ -122,6 +122,61 @@ def test_random_order_vs_oracle(gibbs):
     np.testing.assert_array_equal(bits(e), bits(want_e))
 
 
+def _conflicted_problem(rng, n, degree):
+    """A random problem whose coupler list also repeats about 5% of its pairs
+    (new weights) and holds self-loops, interleaved in input order: the
+    neighbour updates of one pass then name one slot more than once."""
+    h, u, v, J = _random_problem(rng, n, degree=degree)
+    k = max(2, len(u) // 20)
+    idx = rng.integers(0, len(u), k)
+    loops = rng.integers(0, n, k // 2)
+    u = np.concatenate([u, u[idx], loops]).astype(np.int32)
+    v = np.concatenate([v, v[idx], loops]).astype(np.int32)
+    J = np.concatenate([J, rng.normal(0, 1, k), rng.normal(0, 1, k // 2)])
+    order = rng.permutation(len(u))
+    return h, u[order], v[order], J[order]
+
+
+@pytest.mark.parametrize("randomize", [False, True])
+@pytest.mark.parametrize("gibbs", [False, True])
+def test_global_slots_with_repeated_targets_vs_oracle(randomize, gibbs, tmp_path):
+    """n = 2500: above the size the untuned launch keeps on chip, so the delta
+    energies live in global slots and the neighbour additions are L2
+    reductions; repeated couplers and self-loops make several additions to one
+    slot in one pass, which must land in list order.  Untuned, and forced to
+    the location with the spins in global memory too."""
+    rng = np.random.default_rng(71 + 2 * randomize + gibbs)
+    n, R = 2500, 6
+    h, u, v, J = _conflicted_problem(rng, n, 6)
+    st = (2 * rng.integers(0, 2, (R, n)) - 1).astype(np.int8)
+    betas = np.geomspace(0.1, 5.0, 30)
+    seeds = rng.integers(0, 2**63, R).astype(np.uint64)
+    want_s, want_e = oracle.run(h, u, v, J, st, 1, betas, seeds, randomize, gibbs)
+    crit = CRIT[0 if gibbs else 1]
+    stats = {}
+    s, e = simulated_annealing(R, h, u, v, J, 1, betas, 0, st.copy(), randomize, crit,
+                               seeds=seeds, stats=stats)
+    np.testing.assert_array_equal(s, want_s)
+    np.testing.assert_array_equal(bits(e), bits(want_e))
+    assert stats["near_ties"] == 0
+    import torch
+    inst = workloads.Instance(h, u, v, J, st, betas, 1, seeds, randomize, crit)
+    cache = tmp_path / "tune.txt"
+    with Plan([inst]) as plan:
+        plan.autotune(str(cache), force=True)
+    keys = [line.split()[0] for line in cache.read_text().splitlines()]
+    cache.write_text("".join(f"{k} 0 4 0 1 1.0\n" for k in keys))
+    with Plan([inst]) as plan:
+        plan.autotune(str(cache))
+        sin = torch.from_numpy(st.ravel().copy()).cuda()
+        out = torch.empty_like(sin)
+        en = torch.empty(R, dtype=torch.float64, device="cuda")
+        plan.run(sin, out, en, mode="persistent", sync=True)
+        assert all(r["staging"] == 0 for r in plan.bucket_report())
+        np.testing.assert_array_equal(out.cpu().numpy().reshape(R, n), want_s)
+        np.testing.assert_array_equal(bits(en.cpu().numpy()), bits(want_e))
+
+
 def test_shared_stream_matches_reference_multiread():
     rng = np.random.default_rng(9)
     n = 80
