@@ -26,10 +26,11 @@
 // adjacency entries of all committed flips, concatenated in variable order,
 // are spread over the lanes 32 at a time.  Entries that name the same slot
 // (a neighbour shared by two flips, or a self-loop / repeated coupler) are
-// grouped with __match_any_sync and summed by the group's first lane in
-// entry order, so every slot receives its additions in the reference's order.
-// The grouping is skipped when the per-variable conflict masks (computed at
-// pack time) show that no two entries of the pass can name the same slot.
+// grouped with __match_any_sync and added by the group's first lane in entry
+// order, so every slot receives its additions in the reference's order.  The
+// grouping is skipped when the per-variable conflict masks (computed at pack
+// time) show that no two entries of the pass can name the same slot.  Slots in
+// global memory receive their additions as L2 reductions (see GlobalDe).
 #pragma once
 #include <cstdint>
 
