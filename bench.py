@@ -40,10 +40,10 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per attempt of the
 # n ~ 4000 bucket launch with delta energies in per-read global slots, from one
 # ncu capture of the full uneven batch with every schedule cut to 5% of its
-# sweeps: 693.8 GB over 2.26e10 attempts (0.14 bytes read, 30.6 written).  The
+# sweeps: 695.7 GB over 2.26e10 attempts (0.12 bytes read, 30.7 written).  The
 # traffic is per attempt (the schedule length repeats the same sweeps), so a
 # full launch's traffic is this figure times its attempts.
-L2_SLOT_DRAM_BYTES_PER_ATTEMPT = 30.7
+L2_SLOT_DRAM_BYTES_PER_ATTEMPT = 30.8
 
 
 def parse_args():
