@@ -217,6 +217,21 @@ def edge_moments(models: Sequence[IsingModel], samples: Sequence[torch.Tensor],
     return sums_s, sums_ss
 
 
+def pool_sums(sum_s: Sequence[torch.Tensor], sum_ss: Sequence[torch.Tensor], group):
+    """Moment sums added over the ranks of `group`: one all-reduce (NCCL
+    between GPUs) of the concatenated int64 sums, so the pooled sums are
+    exact and identical on every rank.  Returns new lists of the same shapes."""
+    import torch.distributed as dist
+    parts = list(sum_s) + list(sum_ss)
+    flat = torch.cat([x.reshape(-1) for x in parts])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+    out, i = [], 0
+    for x in parts:
+        out.append(flat[i:i + x.numel()].view(x.shape))
+        i += x.numel()
+    return out[:len(sum_s)], out[len(sum_s):]
+
+
 class LogPartition(torch.autograd.Function):
     """``LogPartition.apply(h_cat, J_cat, spec)`` for a batch of models.
 
@@ -225,7 +240,9 @@ class LogPartition(torch.autograd.Function):
     :class:`SamplingSpec`.  Returns a zero placeholder (log Z itself is not
     estimated); the forward's samples are left in ``spec.last_samples``
     (empty when they are recomputed in backward).  Backward returns
-    ``-beta <s_i>`` and ``-beta <s_u s_v>`` per coupler.
+    ``-beta <s_i>`` and ``-beta <s_u s_v>`` per coupler; with ``spec.group``
+    the moments are pooled over the group's ranks (:func:`pool_sums`) before
+    the averages are taken.
     """
 
     @staticmethod
@@ -238,7 +255,8 @@ class LogPartition(torch.autograd.Function):
         keep = spec.reads * sum(m.num_vars for m in spec.models) <= spec.memory_budget
         samples = []
         if keep:
-            samples = spec.sampler(spec.reads).sample_cat(hd, Jd, spec.seed, spec.init_seed, 0)
+            samples = spec.sampler(spec.reads).sample_cat(hd, Jd, spec.seed, spec.init_seed,
+                                                          spec.first_read)
         spec.last_samples = samples
         ctx.spec = spec
         ctx.hs, ctx.Js = hd, Jd
@@ -250,8 +268,10 @@ class LogPartition(torch.autograd.Function):
     def backward(ctx, g):
         spec = ctx.spec
         sum_s, sum_ss = spec.moments(ctx.hs, ctx.Js, ctx.samples)
+        if spec.group is not None:
+            sum_s, sum_ss = pool_sums(sum_s, sum_ss, spec.group)
         spec.last_moments = (sum_s, sum_ss)
-        scale = -spec.beta / spec.reads
+        scale = -spec.beta / spec.total_reads
         gh = (torch.cat([x.to(torch.float64) for x in sum_s]) * scale).to(ctx.h_device)
         gJ = (torch.cat([x.to(torch.float64) for x in sum_ss]) * scale).to(ctx.J_device)
         return gh * g.to(ctx.h_device), gJ * g.to(ctx.J_device), None
@@ -274,6 +294,20 @@ class SamplingSpec:
     last_samples: list = None      # set by LogPartition.forward
     last_moments: tuple = None     # set by LogPartition.backward
     samplers: dict = None          # reads per call -> ModelSampler (plan + graph reused)
+    group: object = None           # torch.distributed group: each rank samples `reads` reads
+
+    @property
+    def first_read(self) -> int:
+        """This rank's first read: with a group, rank k samples reads
+        [k reads, (k + 1) reads) of the pooled set (their seeds and initial
+        states), so the pooled moments equal one run of reads x ranks."""
+        return 0 if self.group is None else torch.distributed.get_rank(self.group) * self.reads
+
+    @property
+    def total_reads(self) -> int:
+        """Reads behind the (pooled) moments."""
+        ranks = 1 if self.group is None else torch.distributed.get_world_size(self.group)
+        return self.reads * ranks
 
     def sampler(self, reads: int) -> ModelSampler:
         """The spec's sampler for calls of `reads` reads (built on first use;
@@ -303,7 +337,8 @@ class SamplingSpec:
         tot_s = tot_ss = None
         for r0 in range(0, self.reads, self.recompute_chunk):
             k = min(self.recompute_chunk, self.reads - r0)
-            chunk = self.sampler(k).sample_cat(h_cat, J_cat, self.seed, self.init_seed, r0)
+            chunk = self.sampler(k).sample_cat(h_cat, J_cat, self.seed, self.init_seed,
+                                               self.first_read + r0)
             s, ss = edge_moments(self.models, chunk, self.device)
             if tot_s is None:
                 tot_s, tot_ss = s, ss

@@ -23,7 +23,7 @@ import numpy as np
 import torch
 
 from .autograd import (IsingModel, ModelSampler, SamplingSpec, edge_moments, log_partition,
-                       sample_models)
+                       pool_sums, sample_models)
 
 
 @dataclass
@@ -40,15 +40,23 @@ class BMResult:
 
 
 def target_correlations(models: Sequence[IsingModel], hs, Js, beta: float, reads: int,
-                        sweeps: int, seed: int, device: int = 0, autotune: bool = False):
+                        sweeps: int, seed: int, device: int = 0, autotune: bool = False,
+                        group=None):
     """<s_u s_v> per coupler of the ground-truth models, from `reads` fixed-beta
-    Gibbs reads of `sweeps` sweeps each."""
+    Gibbs reads of `sweeps` sweeps each (with `group`, `reads` per rank, the
+    sums pooled over the ranks)."""
     sampler = ModelSampler(models, beta, sweeps, reads, "Gibbs", device, autotune)
     try:
-        samples = sample_models(models, hs, Js, beta, sweeps, reads, seed, seed + 1, 0, "Gibbs",
-                                device, sampler)
-        _, sss = edge_moments(models, samples, device)
-        return [x.to(torch.float64) / reads for x in sss]
+        ranks, read0 = 1, 0
+        if group is not None:
+            ranks = torch.distributed.get_world_size(group)
+            read0 = torch.distributed.get_rank(group) * reads
+        samples = sample_models(models, hs, Js, beta, sweeps, reads, seed, seed + 1, read0,
+                                "Gibbs", device, sampler)
+        ss, sss = edge_moments(models, samples, device)
+        if group is not None:
+            _, sss = pool_sums(ss, sss, group)
+        return [x.to(torch.float64) / (reads * ranks) for x in sss]
     finally:
         sampler.close()
 
@@ -57,18 +65,22 @@ def fit(truth: Sequence[tuple], beta: float = 1.0, steps: int = 500, reads: int 
         sweeps: int = 2000, lr: float = 1e-2, target_reads: int = 8192,
         target_sweeps: int = 2000, seed: int = 11, device: int = 0,
         callback: Callable[[int, float], None] | None = None,
-        autotune: bool = True) -> BMResult:
+        autotune: bool = True, group=None) -> BMResult:
     """Fit J (from zero, h fixed at the truth's h) to the truth's coupler
     correlations.  `truth` is a list of (h, u, v, J) ground-truth models.
     With `autotune` the sampling plan's launch shapes are measured once, at
-    the first step (results are the same either way)."""
+    the first step (results are the same either way).  With `group` (a
+    torch.distributed group, one rank per GPU) every rank samples `reads`
+    and `target_reads` reads of every model and the moment sums are pooled
+    by one all-reduce per step, so every rank takes the same Adam step."""
     dev = torch.device("cuda", device)
     models = [IsingModel(len(h), np.ascontiguousarray(u, np.int32), np.ascontiguousarray(v, np.int32))
               for h, u, v, _ in truth]
     hs = [np.asarray(h, np.float64) for h, _, _, _ in truth]
     t0 = time.perf_counter()
     corr_data = target_correlations(models, hs, [np.asarray(J, np.float64) for *_, J in truth],
-                                    beta, target_reads, target_sweeps, seed, device, autotune)
+                                    beta, target_reads, target_sweeps, seed, device, autotune,
+                                    group)
     torch.cuda.synchronize(dev)
     res = BMResult(J=[], target_seconds=time.perf_counter() - t0)
     data = torch.cat(corr_data).to(dev)
@@ -80,13 +92,13 @@ def fit(truth: Sequence[tuple], beta: float = 1.0, steps: int = 500, reads: int 
         t = time.perf_counter()
         spec = SamplingSpec(models, beta=beta, sweeps=sweeps, reads=reads,
                             seed=seed + 1000 + step, init_seed=seed + 7 + step, device=device,
-                            samplers=samplers, autotune=autotune)
+                            samplers=samplers, autotune=autotune, group=group)
         loss = beta * torch.dot(J, data) + log_partition(h_cat, J, spec)
         samplers = spec.samplers
         opt.zero_grad()
         loss.backward()
         opt.step()
-        model_corr = torch.cat([x.to(torch.float64) for x in spec.last_moments[1]]) / reads
+        model_corr = torch.cat([x.to(torch.float64) for x in spec.last_moments[1]]) / spec.total_reads
         err = float(torch.mean(torch.abs(model_corr - data)))
         torch.cuda.synchronize(dev)
         res.step_seconds.append(time.perf_counter() - t)

@@ -157,3 +157,60 @@ def test_device_initial_states_match_host(init_seed, model, read0, reads, n):
     torch.cuda.synchronize()
     np.testing.assert_array_equal(out.cpu().numpy().reshape(reads, n),
                                   initial_states(init_seed, model, reads, n, read0))
+
+
+def _two_models():
+    rng = np.random.default_rng(8)
+    models, hs, Js = [], [], []
+    for k, n in enumerate((40, 70)):
+        n, u, v = workloads.random_regular(n, 3 + k, rng, graph_seed=k + 11)
+        models.append(IsingModel(n, u, v))
+        hs.append(rng.normal(0, 0.1, n))
+        Js.append(rng.normal(0, 0.5, u.shape[0]))
+    return models, np.concatenate(hs), np.concatenate(Js)
+
+
+def _grads(reads, budget, group=None):
+    models, h_cat, J_cat = _two_models()
+    spec = SamplingSpec(models, beta=0.9, sweeps=80, reads=reads, seed=9, init_seed=10,
+                        memory_budget=budget, recompute_chunk=16, group=group)
+    hh = torch.tensor(h_cat, requires_grad=True)
+    JJ = torch.tensor(J_cat, requires_grad=True)
+    log_partition(hh, JJ, spec).backward()
+    return hh.grad.numpy().tolist(), JJ.grad.numpy().tolist()
+
+
+def _pooled_rank(rank, world, port, out):
+    import os
+    import sys
+    from datetime import timedelta
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from conftest import ROOT
+    for p in (ROOT, os.path.join(ROOT, "dwave-samplers_b200")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import torch.distributed as dist
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    out[rank] = [_grads(24, budget, dist.group.WORLD) for budget in (1 << 30, 0)]
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_moments_pooled_over_two_ranks_equal_one_rank_with_all_reads():
+    """Two ranks (processes on one GPU, gloo between them) each sample 24
+    reads of every model (reads [24 k, 24 k + 24) of the pooled set) and pool
+    the moment sums in backward: both hold exactly the gradient of one
+    process sampling all 48 reads, with the samples kept or recomputed."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    want = _grads(48, 1 << 30)
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_pooled_rank, args=(2, port, out), nprocs=2, join=True)
+    for r in range(2):
+        for got in out[r]:
+            assert [list(x) for x in got] == [list(x) for x in want]

@@ -135,3 +135,60 @@ def test_two_rank_sharded_batch_equals_one_rank():
                 assert out[r] == want
             else:
                 assert out[r] is None
+
+
+# ---- Boltzmann-machine moments pooled across ranks (b200sa.autograd) -------
+
+def _bm_problem():
+    rng = np.random.default_rng(91)
+    n = 24
+    iu, ju = np.triu_indices(n, 1)
+    keep = rng.random(iu.shape[0]) < 0.3
+    u, v = iu[keep].astype(np.int32), ju[keep].astype(np.int32)
+    J = rng.normal(0, 0.5, u.shape[0])
+    h = np.zeros(n)
+    states = (2 * rng.integers(0, 2, (16, n)) - 1).astype(np.int8)
+    seeds = np.arange(16, dtype=np.uint64) + 500
+    return h, u, v, J, states, seeds
+
+
+def _bm_sums(rows):
+    """Moment sums (int64) of the oracle's Gibbs reads `rows` at beta = 1."""
+    import oracle
+    h, u, v, J, states, seeds = _bm_problem()
+    s, _ = oracle.run(h, u, v, J, states[rows], 50, np.array([1.0]), seeds[rows], False, True)
+    s = s.astype(np.int64)
+    return s.sum(0), (s[:, u] * s[:, v]).sum(0)
+
+
+def _bm_rank(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    for p in (ROOT, os.path.join(ROOT, "dwave-samplers_b200"), os.path.join(ROOT, "oracle")):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from b200sa.autograd import pool_sums
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    reads = 16 // world  # each rank samples its own reads [rank R, (rank + 1) R)
+    s, ss = _bm_sums(np.arange(rank * reads, (rank + 1) * reads))
+    ps, pss = pool_sums([torch.from_numpy(s)], [torch.from_numpy(ss)], None)
+    out[rank] = (ps[0].numpy().tolist(), pss[0].numpy().tolist())
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_bm_moments_pool_to_the_one_rank_sums():
+    """Each rank takes half of the reads (their seeds and initial states, as a
+    SamplingSpec with a group does) and the moment sums are pooled by one
+    all-reduce: both ranks hold exactly the sums of one run over all reads."""
+    import oracle  # noqa: F401  (built before the ranks start)
+    s, ss = _bm_sums(np.arange(16))
+    world = 2
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_bm_rank, args=(world, _free_port(), out), nprocs=world, join=True)
+    for r in range(world):
+        assert out[r] == (s.tolist(), ss.tolist())
