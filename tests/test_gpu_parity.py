@@ -177,12 +177,12 @@ def test_global_slots_with_repeated_targets_vs_oracle(randomize, gibbs, tmp_path
         np.testing.assert_array_equal(bits(en.cpu().numpy()), bits(want_e))
 
 
-def test_shared_stream_matches_reference_multiread():
+@pytest.mark.parametrize("n", [80, 2500])  # state on chip / in a global slot
+def test_shared_stream_matches_reference_multiread(n):
     rng = np.random.default_rng(9)
-    n = 80
     h, u, v, J = _random_problem(rng, n, degree=4)
     st = (2 * rng.integers(0, 2, (12, n)) - 1).astype(np.int8)
-    betas = np.geomspace(0.1, 4.0, 80)
+    betas = np.geomspace(0.1, 4.0, 80 if n < 1000 else 12)
     want_s, want_e = oracle.run(h, u, v, J, st, 1, betas, [424242], False, False)
     s, e = simulated_annealing(12, h, u, v, J, 1, betas, 424242, st.copy(), rng_stream="shared")
     np.testing.assert_array_equal(s, want_s)
